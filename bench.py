@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark of the photon-mapping hot path on B200.
+
+Metric: kNN radiance queries/s at 1M photons, k=100 — the radiance estimate
+of integrator.h:133-152 (k nearest photons + Lambert BRDF sum) for every
+primary hit of a 512x512x4-spp frame, against a device-resident photon map.
+
+One step = one pass of the estimate over the whole query set (inputs
+already in HBM). L2 is flushed (256 MiB write) before each step, outside
+the step's CUDA events. `e2e` times the same pass through the C ABI entry
+point with pinned host buffers (host->device copy of the queries and the
+device->host copy of the radiance inside the timed region).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun as N independent replicas (the photon map and
+the queries are not exchanged between GPUs; each rank does the full
+pass), timed as the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+K_NEAREST = 100
+N_PHOTONS = 1 << 20
+IMAGE_W = IMAGE_H = 512
+SPP = 4
+BYTES_PER_QUERY = 36 * K_NEAREST + 24  # k photons x 36 B + position in + RGB out
+METRIC = "kNN radiance queries/s at 1M photons k=100"
+CPU_SAMPLE_QUERIES = 40000
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload():
+    from photon_mapping_b200 import workloads as W
+    photons = W.wall_photons(N_PHOTONS, seed=0)
+    queries = W.room_primary_hit_queries(IMAGE_W, IMAGE_H, SPP)
+    return photons, queries
+
+
+def config_dict(nq: int) -> dict:
+    return {
+        "workload": (f"radiance estimate k={K_NEAREST} over a {N_PHOTONS}-photon map on the walls of "
+                     f"the unit Cornell room; queries = primary hits of a {IMAGE_W}x{IMAGE_H}x{SPP}spp "
+                     "frame in pixel order"),
+        "photons": N_PHOTONS,
+        "n_emitted": N_PHOTONS,
+        "k": K_NEAREST,
+        "queries_per_step": nq,
+        "l2": "flushed before every step (256 MiB device write outside the step events)",
+        "parallelism": "replicas",
+    }
+
+
+# ------------------------------------------------------------------ distributed
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def dist_init(world: int, backend: str):
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+# ----------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="clocks_", suffix=".csv")[1])
+
+    def start(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict | None:
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.path.read_text().splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        self.path.unlink(missing_ok=True)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ references
+
+def measured_peak_hbm() -> tuple[float, str]:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return 6650.0, "fallback"
+
+
+def ncu_traffic() -> float | None:
+    """DRAM bytes per launch of the kNN radiance kernel from the committed
+    ncu summary (profiles/knn_radiance_traffic.json), scaled to this
+    workload's query count when the capture ran a smaller case."""
+    p = ROOT / "profiles" / "knn_radiance_traffic.json"
+    if not p.exists():
+        return None
+    try:
+        d = json.loads(p.read_text())
+        return float(d["dram_bytes_per_launch_full_workload"])
+    except Exception:
+        return None
+
+
+def cpu_reference_rate(photons, queries, n_queries: int, repeats: int = 1):
+    """The reference's own photon map + radiance loop (oracle/_ref, compiled
+    from the reference headers) on a bounded sample of the same queries,
+    with every host thread. Returns (queries/s, threads, seconds)."""
+    from oracle import oracle as O
+    if not O.ref_available():
+        return None
+    ref = O.RefPhotonMap(photons)
+    sample = np.ascontiguousarray(queries[:n_queries])
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        ref.radiance(sample, K_NEAREST, N_PHOTONS)
+    dt = time.perf_counter() - t0
+    threads = O.ref_threads()
+    ref.close()
+    return n_queries * repeats / dt, threads, dt
+
+
+# -------------------------------------------------------------------- our arm
+
+def run_ours(args) -> None:
+    import torch
+    world, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = dist_init(world, "nccl")
+    dev = torch.device("cuda", local)
+
+    from photon_mapping_b200 import Context, PhotonMap
+    photons, queries = workload()
+    nq = queries.shape[0]
+    ctx = Context(local)
+    pm = PhotonMap(ctx)
+    pm.setPhotons(photons)
+    pm.build()
+    lib = ctx.lib
+
+    d_q = torch.from_numpy(queries).to(dev)
+    d_out = torch.empty((nq, 3), dtype=torch.float32, device=dev)
+    flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MiB > L2
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        st = lib.pm_photonmap_radiance_device(ctx.handle, 0, d_q.data_ptr(), nq, K_NEAREST,
+                                              N_PHOTONS, d_out.data_ptr(), stream.cuda_stream)
+        ctx.check(st, "pm_photonmap_radiance_device")
+
+    for _ in range(max(args.warmup, 0)):
+        flush.zero_()
+        step()
+    torch.cuda.synchronize(dev)
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    clocks.start()
+    t_wall = time.perf_counter()
+    for e0, e1 in evs:
+        flush.zero_()
+        e0.record(stream)
+        step()
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    t_wall = time.perf_counter() - t_wall
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    times = [e0.elapsed_time(e1) for e0, e1 in evs]
+    ms = sum(times) / len(times)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * nq / (ms / 1e3)
+
+    # e2e through the C ABI with pinned host buffers
+    h_q = torch.from_numpy(queries).pin_memory()
+    h_out = torch.empty((nq, 3), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        st = lib.pm_photonmap_radiance(ctx.handle, 0, h_q.data_ptr(), nq, K_NEAREST, N_PHOTONS,
+                                       h_out.data_ptr())
+        ctx.check(st, "pm_photonmap_radiance")
+
+    for _ in range(max(args.warmup, 1)):
+        e2e_step()
+    if dist:
+        dist.barrier()
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_times.append(time.perf_counter() - t0)
+    e2e_s = sum(e2e_times) / len(e2e_times)
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * nq / e2e_s
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = cpu_reference_rate(photons, queries, CPU_SAMPLE_QUERIES)
+        if r:
+            rate, threads, secs = r
+            cpu = {"value": rate, "unit": "queries/s", "cores": threads, "kind": "reference",
+                   "sample": (f"{CPU_SAMPLE_QUERIES} of the {nq} queries through the reference's "
+                              f"PhotonMap + radiance loop (photon_map.h, integrator.h:133-152 "
+                              f"compiled with g++ -O3 -fopenmp), {secs:.1f} s")}
+
+    peak, peak_kind = measured_peak_hbm()
+    achieved = nq * BYTES_PER_QUERY / (ms / 1e3) / 1e9
+    traffic = ncu_traffic()
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded photon set on the Cornell walls; primary-hit queries)",
+        "config": config_dict(nq),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "bytes_per_query": BYTES_PER_QUERY},
+        "cpu_baseline": cpu,
+        "e2e": {"value": e2e_value, "unit": "queries/s",
+                "h2d_bytes_per_step": int(queries.nbytes),
+                "d2h_bytes_per_step": int(nq * 3 * 4)},
+        "gpu_launches": args.steps,
+        "clocks": clk,
+        "wall_s_timed_region": t_wall,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# -------------------------------------------------------------- reference arm
+
+def run_reference(args) -> None:
+    world, rank, local = dist_env()
+    if rank != 0:
+        return
+    from oracle import oracle as O
+    if not O.ref_available():
+        try:
+            O.build()
+        except Exception as e:  # pragma: no cover
+            print(json.dumps({"impl": "reference", "unavailable": f"reference build failed: {e}"}))
+            return
+    photons, queries = workload()
+    nq = queries.shape[0]
+    ref = O.RefPhotonMap(photons)
+    sample = np.ascontiguousarray(queries[:CPU_SAMPLE_QUERIES // 2])
+    for _ in range(max(args.warmup, 0)):
+        ref.radiance(sample[:2000], K_NEAREST, N_PHOTONS)
+    times = []
+    for s in range(args.steps):
+        off = (s * sample.shape[0]) % max(nq - sample.shape[0], 1)
+        chunk = np.ascontiguousarray(queries[off: off + sample.shape[0]])
+        t0 = time.perf_counter()
+        ref.radiance(chunk, K_NEAREST, N_PHOTONS)
+        times.append(time.perf_counter() - t0)
+    threads = O.ref_threads()
+    ref.close()
+    secs = sum(times) / len(times)
+    value = sample.shape[0] / secs
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "queries/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": secs * 1e3,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded photon set on the Cornell walls; primary-hit queries)",
+        "config": config_dict(nq),
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "reference",
+                         "sample": (f"{sample.shape[0]} queries per step through the reference's "
+                                    "PhotonMap + radiance loop (g++ -O3 -fopenmp)")},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,150 @@
+"""ORACLE — test infrastructure only.
+
+ctypes access to the CPU restatement (``_build/liboracle.so``) and to the
+reference's own code compiled unchanged (``_ref/*.so``). Only tests/,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py use this
+module; the product never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "liboracle.so"
+REF_PM_SO = HERE / "_ref" / "libpmref_photonmap.so"
+
+_i64, _vp = C.c_int64, C.c_void_p
+
+
+def build() -> None:
+    r = subprocess.run(["make", "-s", "-C", str(HERE)], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"oracle build failed:\n{r.stdout}\n{r.stderr}")
+
+
+def _load(path: Path, sigs: dict) -> C.CDLL:
+    if not path.exists():
+        build()
+    lib = C.CDLL(str(path))
+    for name, (res, args) in sigs.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_oracle = None
+_refpm = None
+
+
+def oracle_lib() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        _oracle = _load(ORACLE_SO, {
+            "orc_knn": (None, [_vp, _i64, _vp, _i64, C.c_int, _vp, _vp, _vp]),
+            "orc_radiance_fp64": (None, [_vp, _vp, _vp, _vp, C.c_int, _vp, _i64, _i64, _vp]),
+            "orc_radiance_fp32": (None, [_vp, _vp, _vp, _vp, C.c_int, _vp, _i64, _i64, _vp]),
+        })
+    return _oracle
+
+
+def ref_available() -> bool:
+    return REF_PM_SO.exists()
+
+
+def ref_pm_lib() -> C.CDLL:
+    global _refpm
+    if _refpm is None:
+        _refpm = _load(REF_PM_SO, {
+            "ref_pm_build": (_vp, [_vp, _i64]),
+            "ref_pm_free": (None, [_vp]),
+            "ref_max_threads": (C.c_int, []),
+            "ref_pm_knn": (None, [_vp, _vp, _i64, C.c_int, _vp, _vp, _vp]),
+            "ref_pm_radiance": (None, [_vp, _vp, _i64, C.c_int, C.c_int, _vp]),
+        })
+    return _refpm
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype))
+
+
+def knn(photons, queries, k: int):
+    """Exact kNN by brute force: (idx (nq,k) in heap-pop order, count, maxdist2)."""
+    ph = _c(photons, np.float32).reshape(-1, 9)
+    q = _c(queries, np.float32).reshape(-1, 3)
+    nq = q.shape[0]
+    idx = np.empty((nq, k), np.int32)
+    cnt = np.empty(nq, np.int32)
+    md2 = np.empty(nq, np.float32)
+    oracle_lib().orc_knn(ph.ctypes.data, ph.shape[0], q.ctypes.data, nq, k,
+                         idx.ctypes.data, cnt.ctypes.data, md2.ctypes.data)
+    return idx, cnt, md2
+
+
+def radiance_fp64(photons, idx, cnt, md2, queries, n_emitted: int) -> np.ndarray:
+    ph = _c(photons, np.float32).reshape(-1, 9)
+    idx, cnt, md2 = _c(idx, np.int32), _c(cnt, np.int32), _c(md2, np.float32)
+    q = _c(queries, np.float32).reshape(-1, 12)
+    out = np.empty((q.shape[0], 3), np.float64)
+    oracle_lib().orc_radiance_fp64(ph.ctypes.data, idx.ctypes.data, cnt.ctypes.data,
+                                   md2.ctypes.data, idx.shape[1], q.ctypes.data,
+                                   q.shape[0], int(n_emitted), out.ctypes.data)
+    return out
+
+
+def radiance_fp32(photons, idx, cnt, md2, queries, n_emitted: int) -> np.ndarray:
+    ph = _c(photons, np.float32).reshape(-1, 9)
+    idx, cnt, md2 = _c(idx, np.int32), _c(cnt, np.int32), _c(md2, np.float32)
+    q = _c(queries, np.float32).reshape(-1, 12)
+    out = np.empty((q.shape[0], 3), np.float32)
+    oracle_lib().orc_radiance_fp32(ph.ctypes.data, idx.ctypes.data, cnt.ctypes.data,
+                                   md2.ctypes.data, idx.shape[1], q.ctypes.data,
+                                   q.shape[0], int(n_emitted), out.ctypes.data)
+    return out
+
+
+class RefPhotonMap:
+    """The reference's PhotonMap (photon_map.h), compiled unchanged."""
+
+    def __init__(self, photons):
+        self.lib = ref_pm_lib()
+        self.ph = _c(photons, np.float32).reshape(-1, 9)
+        self.h = self.lib.ref_pm_build(self.ph.ctypes.data, self.ph.shape[0])
+
+    def knn(self, queries, k: int):
+        q = _c(queries, np.float32).reshape(-1, 3)
+        nq = q.shape[0]
+        idx = np.empty((nq, k), np.int32)
+        cnt = np.empty(nq, np.int32)
+        md2 = np.empty(nq, np.float32)
+        self.lib.ref_pm_knn(self.h, q.ctypes.data, nq, k, idx.ctypes.data,
+                            cnt.ctypes.data, md2.ctypes.data)
+        return idx, cnt, md2
+
+    def radiance(self, queries, k: int, n_emitted: int) -> np.ndarray:
+        q = _c(queries, np.float32).reshape(-1, 12)
+        out = np.empty((q.shape[0], 3), np.float32)
+        self.lib.ref_pm_radiance(self.h, q.ctypes.data, q.shape[0], k, int(n_emitted),
+                                 out.ctypes.data)
+        return out
+
+    def close(self):
+        if self.h:
+            self.lib.ref_pm_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_threads() -> int:
+    return int(ref_pm_lib().ref_max_threads())

@@ -1,0 +1,65 @@
+// Shared device helpers of libpm_cuda.
+//
+// All device code of this library is compiled with -fmad=false: every
+// float expression rounds after each operation, exactly like the
+// reference's x86-64 build (SSE scalar math, no FMA contraction), so
+// distances, dot products and normalisations are bit-identical to the
+// reference arithmetic written in the same order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pm {
+
+constexpr int kWarp = 32;
+constexpr unsigned kFull = 0xffffffffu;
+
+// core.h:7 — PI is the double literal 3.14159265359 rounded to float.
+constexpr float kPI = 3.14159265359f;
+// core.h:19
+constexpr float kRayEps = 1e-5f;
+
+__device__ __forceinline__ unsigned lane_id() {
+  unsigned l;
+  asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
+  return l;
+}
+__device__ __forceinline__ unsigned lanemask_lt() {
+  unsigned m;
+  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+
+// Squared distance in the reference order: ((dx*dx) + dy*dy) + dz*dz with
+// d = q - p (photon_map.h:33-41; 0 + a == a exactly).
+__device__ __forceinline__ float dist2_ref(float qx, float qy, float qz,
+                                           float px, float py, float pz) {
+  const float dx = qx - px, dy = qy - py, dz = qz - pz;
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)),
+                   __fmul_rn(dz, dz));
+}
+
+// dot() of core.h:200-203: (a0*b0 + a1*b1) + a2*b2, rounded per operation.
+__device__ __forceinline__ float dot_ref(float a0, float a1, float a2,
+                                         float b0, float b1, float b2) {
+  return __fadd_rn(__fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1)),
+                   __fmul_rn(a2, b2));
+}
+
+// Lower bound of dist2_ref(q, p) over every p inside the box [lo, hi]:
+// each axis term uses the same subtraction and rounding as dist2_ref, and
+// IEEE rounding is monotone, so the result never exceeds the distance the
+// kernel computes for any photon inside the box.
+__device__ __forceinline__ float box_dist2(float qx, float qy, float qz,
+                                           const float4& lo,
+                                           const float4& hi) {
+  float dx = 0.f, dy = 0.f, dz = 0.f;
+  if (qx < lo.x) dx = lo.x - qx; else if (qx > hi.x) dx = qx - hi.x;
+  if (qy < lo.y) dy = lo.y - qy; else if (qy > hi.y) dy = qy - hi.y;
+  if (qz < lo.z) dz = lo.z - qz; else if (qz > hi.z) dz = qz - hi.z;
+  return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)),
+                   __fmul_rn(dz, dz));
+}
+
+}  // namespace pm

@@ -1,0 +1,695 @@
+// Photon map on the device: build (Morton order + 32-ary box tree) and the
+// warp-per-query k-nearest-neighbour search with the radiance estimate.
+//
+// Reference behaviour followed here (yumcyaWiz/photon_mapping):
+//   photon_map.h:33-41    distance2: float sum of squared differences x,y,z
+//   photon_map.h:107-147  kNN search keeping the k smallest (dist2, index)
+//                         pairs (std::priority_queue of pair<float,int>,
+//                         so among equal distances the smaller index wins)
+//   photon_map.h:166-183  result order (heap pops: largest pair first) and
+//                         maxDist2 = largest kept dist2
+//   integrator.h:133-152  radiance estimate with the Lambert BRDF
+//   material.h:80-88      Lambert::evaluate
+#include "pm_photonmap.cuh"
+#include "pm_sort.cuh"
+
+#include <float.h>
+
+namespace pm {
+
+// ------------------------------------------------------------------ build
+
+int map_levels(int64_t n, int* nlevels, int* lvl_off, int* lvl_cnt) {
+  if (n <= 0) {
+    *nlevels = 0;
+    return 0;
+  }
+  int64_t cnt = (n + 31) / 32;
+  int lv = 0, off = 0;
+  while (true) {
+    lvl_off[lv] = off;
+    lvl_cnt[lv] = (int)cnt;
+    off += (int)cnt;
+    ++lv;
+    if (cnt == 1) break;
+    cnt = (cnt + 31) / 32;
+  }
+  *nlevels = lv;
+  return off;
+}
+
+size_t map_build_scratch_bytes(int64_t n) {
+  const size_t nn = (size_t)(n > 0 ? n : 1);
+  // keys a/b, values a/b, tile histogram, bbox words
+  return 4 * nn * sizeof(uint32_t) + 256 * (size_t)sort_tiles(nn) * 4 + 64;
+}
+
+__device__ __forceinline__ uint32_t ordered_bits(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float from_ordered(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__global__ void bbox_kernel(const float* __restrict__ aos, int n,
+                            uint32_t* __restrict__ bb) {
+  float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
+  float hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const float v = aos[9 * (size_t)i + 3 + a];
+      lo[a] = fminf(lo[a], v);  // fminf ignores NaN
+      hi[a] = fmaxf(hi[a], v);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      lo[a] = fminf(lo[a], __shfl_xor_sync(kFull, lo[a], o));
+      hi[a] = fmaxf(hi[a], __shfl_xor_sync(kFull, hi[a], o));
+    }
+  }
+  if ((threadIdx.x & 31) == 0) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      atomicMin(&bb[a], ordered_bits(lo[a]));
+      atomicMax(&bb[3 + a], ordered_bits(hi[a]));
+    }
+  }
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t x) {
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+__device__ __forceinline__ uint32_t cell10(float v, float lo, float ext) {
+  if (!(ext > 0.f)) return 0;
+  float t = (v - lo) / ext * 1024.f;
+  if (!(t > 0.f)) return 0;  // also NaN
+  return t >= 1023.f ? 1023u : (uint32_t)t;
+}
+
+__global__ void morton_kernel(const float* __restrict__ aos, int n,
+                              const uint32_t* __restrict__ bb,
+                              uint32_t* __restrict__ keys,
+                              uint32_t* __restrict__ vals) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float lo[3], ext[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = from_ordered(bb[a]);
+    ext[a] = from_ordered(bb[3 + a]) - lo[a];
+  }
+  const float* p = aos + 9 * (size_t)i + 3;
+  const uint32_t cx = cell10(p[0], lo[0], ext[0]);
+  const uint32_t cy = cell10(p[1], lo[1], ext[1]);
+  const uint32_t cz = cell10(p[2], lo[2], ext[2]);
+  keys[i] = (spread10(cx) << 2) | (spread10(cy) << 1) | spread10(cz);
+  vals[i] = (uint32_t)i;
+}
+
+__global__ void gather_kernel(const float* __restrict__ aos, int n,
+                              const uint32_t* __restrict__ order,
+                              float4* __restrict__ pos4,
+                              float4* __restrict__ thr4,
+                              float2* __restrict__ wi2) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t i = order[s];
+  const float* r = aos + 9 * (size_t)i;
+  pos4[s] = make_float4(r[3], r[4], r[5], __uint_as_float(i));
+  thr4[s] = make_float4(r[0], r[1], r[2], r[6]);
+  wi2[s] = make_float2(r[7], r[8]);
+}
+
+__global__ void leaf_box_kernel(const float4* __restrict__ pos4, int n,
+                                int nleaves, float4* __restrict__ boxes) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= nleaves) return;
+  const int i = warp * 32 + lane;
+  float4 lo = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
+  float4 hi = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, 0.f);
+  if (i < n) {
+    const float4 p = pos4[i];
+    lo.x = fminf(lo.x, p.x); lo.y = fminf(lo.y, p.y); lo.z = fminf(lo.z, p.z);
+    hi.x = fmaxf(hi.x, p.x); hi.y = fmaxf(hi.y, p.y); hi.z = fmaxf(hi.z, p.z);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = fminf(lo.x, __shfl_xor_sync(kFull, lo.x, o));
+    lo.y = fminf(lo.y, __shfl_xor_sync(kFull, lo.y, o));
+    lo.z = fminf(lo.z, __shfl_xor_sync(kFull, lo.z, o));
+    hi.x = fmaxf(hi.x, __shfl_xor_sync(kFull, hi.x, o));
+    hi.y = fmaxf(hi.y, __shfl_xor_sync(kFull, hi.y, o));
+    hi.z = fmaxf(hi.z, __shfl_xor_sync(kFull, hi.z, o));
+  }
+  if (lane == 0) {
+    boxes[2 * warp] = lo;
+    boxes[2 * warp + 1] = hi;
+  }
+}
+
+__global__ void node_box_kernel(float4* __restrict__ boxes, int child_off,
+                                int child_cnt, int node_off, int node_cnt) {
+  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (warp >= node_cnt) return;
+  const int c = warp * 32 + lane;
+  float4 lo = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
+  float4 hi = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, 0.f);
+  if (c < child_cnt) {
+    const float4 a = boxes[2 * (child_off + c)];
+    const float4 b = boxes[2 * (child_off + c) + 1];
+    lo.x = a.x; lo.y = a.y; lo.z = a.z;
+    hi.x = b.x; hi.y = b.y; hi.z = b.z;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo.x = fminf(lo.x, __shfl_xor_sync(kFull, lo.x, o));
+    lo.y = fminf(lo.y, __shfl_xor_sync(kFull, lo.y, o));
+    lo.z = fminf(lo.z, __shfl_xor_sync(kFull, lo.z, o));
+    hi.x = fmaxf(hi.x, __shfl_xor_sync(kFull, hi.x, o));
+    hi.y = fmaxf(hi.y, __shfl_xor_sync(kFull, hi.y, o));
+    hi.z = fmaxf(hi.z, __shfl_xor_sync(kFull, hi.z, o));
+  }
+  if (lane == 0) {
+    boxes[2 * (node_off + warp)] = lo;
+    boxes[2 * (node_off + warp) + 1] = hi;
+  }
+}
+
+void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
+                      float2* wi2, float4* boxes, const int* lvl_off,
+                      const int* lvl_cnt, int nlevels, void* scratch,
+                      cudaStream_t st) {
+  if (n <= 0) return;
+  uint32_t* ka = (uint32_t*)scratch;
+  uint32_t* kb = ka + n;
+  uint32_t* va = kb + n;
+  uint32_t* vb = va + n;
+  uint32_t* hist = vb + n;
+  uint32_t* bb = hist + 256 * (size_t)sort_tiles(n);
+  cudaMemsetAsync(bb, 0xff, 3 * sizeof(uint32_t), st);
+  cudaMemsetAsync(bb + 3, 0x00, 3 * sizeof(uint32_t), st);
+  const int tb = 256;
+  const int gb = (n + tb - 1) / tb;
+  bbox_kernel<<<min(gb, 1184), tb, 0, st>>>(aos, n, bb);
+  morton_kernel<<<gb, tb, 0, st>>>(aos, n, bb, ka, va);
+  const bool in_b = radix_sort_pairs<uint32_t>(ka, va, kb, vb, n, 30, hist, st);
+  gather_kernel<<<gb, tb, 0, st>>>(aos, n, in_b ? vb : va, pos4, thr4, wi2);
+  const int nleaves = lvl_cnt[0];
+  leaf_box_kernel<<<(nleaves * 32 + tb - 1) / tb, tb, 0, st>>>(pos4, n, nleaves,
+                                                               boxes);
+  for (int l = 1; l < nlevels; ++l) {
+    node_box_kernel<<<(lvl_cnt[l] * 32 + tb - 1) / tb, tb, 0, st>>>(
+        boxes, lvl_off[l - 1], lvl_cnt[l - 1], lvl_off[l], lvl_cnt[l]);
+  }
+}
+
+// -------------------------------------------------------------- kNN query
+
+constexpr int kStack = 256;  // 32 entries per tree level, 8 levels
+constexpr int kChunk = 32;   // queries a warp takes per work-counter bump
+
+template <int C>
+struct WarpBuf {
+  uint32_t key[C];  // float bits of dist2 (non-negative: order == uint order)
+  uint32_t id[C];   // sorted position of the photon
+  uint32_t hist[256];
+  uint32_t stack[kStack];
+};
+
+__device__ __forceinline__ uint32_t orig_index(const MapDev& m, uint32_t s) {
+  return __float_as_uint(m.pos4[s].w);
+}
+
+// k-th smallest (1-based) value among the valid entries i in [0, cnt),
+// `get(i, v)` giving validity and value. Radix select over 8-bit digits
+// (MSB first) with a 256-bin shared histogram; digits common to all values
+// are skipped. Returns the value; *rank_eq = rank still needed among the
+// entries equal to it (>= 1), *n_eq = how many entries equal it.
+// Precondition: 1 <= kk <= number of valid entries.
+template <class Get>
+__device__ uint32_t warp_select(uint32_t* hist, int cnt, uint32_t kk, Get get,
+                                int lane, uint32_t* rank_eq, uint32_t* n_eq) {
+  uint32_t vor = 0, vand = 0xffffffffu, nvalid = 0;
+  for (int i = lane; i < cnt; i += 32) {
+    uint32_t v;
+    if (get(i, v)) {
+      vor |= v;
+      vand &= v;
+      ++nvalid;
+    }
+  }
+  vor = __reduce_or_sync(kFull, vor);
+  vand = __reduce_and_sync(kFull, vand);
+  const uint32_t diff = vor ^ vand;
+  if (diff == 0) {
+    *rank_eq = kk;
+    *n_eq = __reduce_add_sync(kFull, nvalid);
+    return vand;
+  }
+  const int top = 31 - __clz(diff);
+  int shift = (top / 8) * 8;
+  const uint64_t above = ~((1ull << (shift + 8)) - 1ull);
+  uint32_t pmask = (uint32_t)above;
+  uint32_t prefix = vand & pmask;
+  uint32_t last = 0;
+#pragma unroll 1
+  for (; shift >= 0; shift -= 8) {
+    for (int b = lane; b < 256; b += 32) hist[b] = 0;
+    __syncwarp();
+    for (int i = lane; i < cnt; i += 32) {
+      uint32_t v;
+      if (get(i, v) && (v & pmask) == prefix)
+        atomicAdd(&hist[(v >> shift) & 255u], 1u);
+    }
+    __syncwarp();
+    uint32_t h[8];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      h[j] = hist[lane * 8 + j];
+      sum += h[j];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += t;
+    }
+    const uint32_t excl = incl - sum;
+    const unsigned owner = __ballot_sync(kFull, excl < kk && kk <= incl);
+    const int ol = __ffs(owner) - 1;
+    uint32_t digit = 0, nk = 0, cd = 0;
+    if (lane == ol) {
+      uint32_t run = excl;
+      bool found = false;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        if (!found) {
+          if (run + h[j] >= kk) {
+            digit = (uint32_t)(lane * 8 + j);
+            nk = kk - run;
+            cd = h[j];
+            found = true;
+          } else {
+            run += h[j];
+          }
+        }
+      }
+    }
+    digit = __shfl_sync(kFull, digit, ol);
+    kk = __shfl_sync(kFull, nk, ol);
+    last = __shfl_sync(kFull, cd, ol);
+    prefix |= digit << shift;
+    pmask |= 255u << shift;
+    __syncwarp();
+  }
+  *rank_eq = kk;
+  *n_eq = last;
+  return prefix;
+}
+
+// Exact k-th smallest (dist2, index) pair of the buffer: kth_key, and
+// kth_oid = largest original index kept among entries with key == kth_key
+// (0xffffffff when all of them are kept).
+template <int C>
+__device__ void select_kth(const MapDev& m, WarpBuf<C>& s, int cnt, int k,
+                           int lane, uint32_t& kth_key, uint32_t& kth_oid) {
+  uint32_t rank_eq, n_eq;
+  kth_key = warp_select(
+      s.hist, cnt, (uint32_t)k,
+      [&](int i, uint32_t& v) {
+        v = s.key[i];
+        return true;
+      },
+      lane, &rank_eq, &n_eq);
+  kth_oid = 0xffffffffu;
+  if (rank_eq != n_eq) {
+    uint32_t r2, n2;
+    const uint32_t kk = kth_key;
+    kth_oid = warp_select(
+        s.hist, cnt, rank_eq,
+        [&](int i, uint32_t& v) {
+          if (s.key[i] != kk) return false;
+          v = orig_index(m, s.id[i]);
+          return true;
+        },
+        lane, &r2, &n2);
+  }
+}
+
+__device__ __forceinline__ bool keep_entry(const MapDev& m, uint32_t key,
+                                           uint32_t id, uint32_t kth_key,
+                                           uint32_t kth_oid) {
+  if (key < kth_key) return true;
+  if (key != kth_key) return false;
+  return kth_oid == 0xffffffffu || orig_index(m, id) <= kth_oid;
+}
+
+template <int C>
+__device__ int compact_kept(const MapDev& m, WarpBuf<C>& s, int cnt,
+                            uint32_t kth_key, uint32_t kth_oid, int lane) {
+  int dst = 0;
+  for (int b = 0; b < cnt; b += 32) {
+    const int i = b + lane;
+    const bool v = i < cnt;
+    const uint32_t key = v ? s.key[i] : 0u;
+    const uint32_t id = v ? s.id[i] : 0u;
+    const bool kp = v && keep_entry(m, key, id, kth_key, kth_oid);
+    const unsigned bal = __ballot_sync(kFull, kp);
+    __syncwarp();
+    if (kp) {
+      const int o = dst + __popc(bal & lanemask_lt());
+      s.key[o] = key;
+      s.id[o] = id;
+    }
+    dst += __popc(bal);
+  }
+  __syncwarp();
+  return dst;
+}
+
+// Appends every photon of `leaf` with dist2 <= tau. When the buffer is
+// nearly full, keeps only the k best and lowers tau to the k-th distance.
+template <int C>
+__device__ __forceinline__ void scan_leaf(const MapDev& m, int leaf, float qx,
+                                          float qy, float qz, float& tau,
+                                          int& cnt, WarpBuf<C>& s, int lane,
+                                          int k) {
+  const int i = leaf * 32 + lane;
+  const bool ok = i < m.n;
+  float d2 = 0.f;
+  if (ok) {
+    const float4 p = __ldg(m.pos4 + i);
+    d2 = dist2_ref(qx, qy, qz, p.x, p.y, p.z);
+  }
+  const bool pass = ok && d2 <= tau;
+  const unsigned bal = __ballot_sync(kFull, pass);
+  if (pass) {
+    const int o = cnt + __popc(bal & lanemask_lt());
+    s.key[o] = __float_as_uint(d2);
+    s.id[o] = (uint32_t)i;
+  }
+  cnt += __popc(bal);
+  if (cnt > C - 32) {
+    __syncwarp();
+    uint32_t kth_key, kth_oid;
+    select_kth(m, s, cnt, k, lane, kth_key, kth_oid);
+    cnt = compact_kept(m, s, cnt, kth_key, kth_oid, lane);
+    tau = __uint_as_float(kth_key);
+  }
+}
+
+// Depth-first walk of the box tree collecting all photons with dist2 <= tau.
+template <int C>
+__device__ int collect(const MapDev& m, float qx, float qy, float qz,
+                       float& tau, WarpBuf<C>& s, int lane, int k) {
+  int cnt = 0;
+  const int top = m.nlevels - 1;
+  if (lane == 0) s.stack[0] = ((uint32_t)top << 28);
+  int sp = 1;
+  __syncwarp();
+  while (sp > 0) {
+    --sp;
+    const uint32_t e = s.stack[sp];
+    __syncwarp();
+    const int lvl = (int)(e >> 28);
+    const int node = (int)(e & 0x0fffffffu);
+    if (lvl == 0) {
+      scan_leaf(m, node, qx, qy, qz, tau, cnt, s, lane, k);
+      continue;
+    }
+    const int cl = lvl - 1;
+    const int c = node * 32 + lane;
+    bool pass = false;
+    if (c < m.lvl_cnt[cl]) {
+      const int j = m.lvl_off[cl] + c;
+      const float4 lo = __ldg(m.boxes + 2 * j);
+      const float4 hi = __ldg(m.boxes + 2 * j + 1);
+      pass = box_dist2(qx, qy, qz, lo, hi) <= tau;
+    }
+    unsigned bal = __ballot_sync(kFull, pass);
+    if (cl == 0) {
+      while (bal) {
+        const int b = __ffs(bal) - 1;
+        bal &= bal - 1;
+        scan_leaf(m, node * 32 + b, qx, qy, qz, tau, cnt, s, lane, k);
+      }
+    } else {
+      if (pass)
+        s.stack[sp + __popc(bal & lanemask_lt())] = ((uint32_t)cl << 28) | c;
+      sp += __popc(bal);
+      __syncwarp();
+    }
+  }
+  return cnt;
+}
+
+__device__ __forceinline__ unsigned long long warp_min_u64(
+    unsigned long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    const unsigned long long t = __shfl_xor_sync(kFull, v, o);
+    v = t < v ? t : v;
+  }
+  return v;
+}
+
+// Upper bound of the k-th distance from scratch: walk down to the nearest
+// box greedily, then take the k-th distance among the photons of the
+// leaves around it (real photons, so the bound is valid).
+template <int C>
+__device__ float cold_tau(const MapDev& m, float qx, float qy, float qz,
+                          WarpBuf<C>& s, int lane, int k) {
+  int node = 0;
+  for (int lvl = m.nlevels - 1; lvl >= 1; --lvl) {
+    const int cl = lvl - 1;
+    const int c = node * 32 + lane;
+    unsigned long long key = ~0ull;
+    if (c < m.lvl_cnt[cl]) {
+      const int j = m.lvl_off[cl] + c;
+      const float d = box_dist2(qx, qy, qz, __ldg(m.boxes + 2 * j),
+                                __ldg(m.boxes + 2 * j + 1));
+      key = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)c;
+    }
+    key = warp_min_u64(key);
+    node = (int)(key & 0xffffffffu);
+  }
+  const int nleaves = m.lvl_cnt[0];
+  const int want = min(nleaves, (k + 31) / 32 + 2);
+  const int first = max(0, min(node - want / 2, nleaves - want));
+  float tau = __int_as_float(0x7f800000);  // +inf
+  int cnt = 0;
+  for (int l = first; l < first + want; ++l)
+    scan_leaf(m, l, qx, qy, qz, tau, cnt, s, lane, k);
+  __syncwarp();
+  if (cnt < k) return __int_as_float(0x7f800000);
+  uint32_t kth_key, kth_oid;
+  select_kth(m, s, cnt, k, lane, kth_key, kth_oid);
+  return __uint_as_float(kth_key);
+}
+
+template <int C, int MODE>
+__global__ void __launch_bounds__(256)
+    knn_kernel(MapDev m, const void* __restrict__ queries, int64_t nq, int k,
+               float n_emitted, KnnOut out,
+               unsigned long long* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpBuf<C>& s = reinterpret_cast<WarpBuf<C>*>(smem_raw)[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const float kInf = __int_as_float(0x7f800000);
+
+  while (true) {
+    unsigned long long c0 = 0;
+    if (lane == 0) c0 = atomicAdd(counter, 1ull);
+    c0 = __shfl_sync(kFull, c0, 0);
+    const int64_t qb = (int64_t)c0 * kChunk;
+    if (qb >= nq) break;
+    const int64_t qe = min(nq, qb + kChunk);
+
+    bool have_prev = false;
+    float pqx = 0.f, pqy = 0.f, pqz = 0.f, pkth = 0.f;
+    for (int64_t qi = qb; qi < qe; ++qi) {
+      float qx, qy, qz;
+      // radiance records: r0 = {pos, rho.r}, r1 = {wo, rho.g},
+      // r2 = {ns, rho.b}
+      float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0, r2 = r0;
+      if (MODE == kModeRadiance) {
+        const float4* q4 = reinterpret_cast<const float4*>(queries) + 3 * qi;
+        r0 = __ldg(q4);
+        r1 = __ldg(q4 + 1);
+        r2 = __ldg(q4 + 2);
+        qx = r0.x; qy = r0.y; qz = r0.z;
+      } else {
+        const float* q3 = reinterpret_cast<const float*>(queries) + 3 * qi;
+        qx = __ldg(q3);
+        qy = __ldg(q3 + 1);
+        qz = __ldg(q3 + 2);
+      }
+
+      int cnt = 0;
+      float tau = kInf;
+      const bool bad = m.n == 0 || isnan(qx) || isnan(qy) || isnan(qz);
+      if (!bad) {
+        bool warm = false;
+        if (have_prev) {
+          const float d2 = dist2_ref(qx, qy, qz, pqx, pqy, pqz);
+          if (d2 <= pkth) {
+            const float r = sqrtf(pkth) + sqrtf(d2);
+            const float rr = r * 1.00001f;
+            tau = fmaxf(rr * rr * 1.00001f, 1e-37f);
+            warm = true;
+          }
+        }
+        if (!warm) tau = cold_tau(m, qx, qy, qz, s, lane, k);
+        cnt = collect(m, qx, qy, qz, tau, s, lane, k);
+      }
+      __syncwarp();
+
+      // final selection
+      const bool all = cnt <= k;
+      uint32_t kth_key = 0, kth_oid = 0xffffffffu;
+      if (all) {
+        uint32_t mx = 0;
+        for (int i = lane; i < cnt; i += 32) mx = max(mx, s.key[i]);
+        kth_key = __reduce_max_sync(kFull, mx);
+      } else {
+        select_kth(m, s, cnt, k, lane, kth_key, kth_oid);
+      }
+      const int kept = all ? cnt : k;
+      const float maxd2 = kept > 0 ? __uint_as_float(kth_key) : 0.f;
+
+      if (MODE == kModeRadiance) {
+        const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
+        const float fr = __fdiv_rn(r0.w, kPI);
+        const float fg = __fdiv_rn(r1.w, kPI);
+        const float fb = __fdiv_rn(r2.w, kPI);
+        float lr = 0.f, lg = 0.f, lb = 0.f;
+        for (int i = lane; i < cnt; i += 32) {
+          const uint32_t key = s.key[i];
+          const uint32_t id = s.id[i];
+          if (all || keep_entry(m, key, id, kth_key, kth_oid)) {
+            const float4 t = __ldg(m.thr4 + id);
+            const float2 w = __ldg(m.wi2 + id);
+            const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
+            // Lambert::evaluate returns 0 when either cosine is < 0
+            if (!(cos_o < 0.f) && !(cos_i < 0.f)) {
+              lr = __fadd_rn(lr, __fmul_rn(fr, t.x));
+              lg = __fadd_rn(lg, __fmul_rn(fg, t.y));
+              lb = __fadd_rn(lb, __fmul_rn(fb, t.z));
+            }
+          }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          lr = __fadd_rn(lr, __shfl_xor_sync(kFull, lr, o));
+          lg = __fadd_rn(lg, __shfl_xor_sync(kFull, lg, o));
+          lb = __fadd_rn(lb, __shfl_xor_sync(kFull, lb, o));
+        }
+        if (lane == 0) {
+          float3 o3 = make_float3(0.f, 0.f, 0.f);
+          if (kept > 0) {
+            const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
+            o3 = make_float3(__fdiv_rn(lr, den), __fdiv_rn(lg, den),
+                             __fdiv_rn(lb, den));
+          }
+          out.rgb[3 * qi + 0] = o3.x;
+          out.rgb[3 * qi + 1] = o3.y;
+          out.rgb[3 * qi + 2] = o3.z;
+        }
+      } else {
+        int n2 = cnt;
+        if (!all) n2 = compact_kept(m, s, cnt, kth_key, kth_oid, lane);
+        for (int i = lane; i < n2; i += 32) s.id[i] = orig_index(m, s.id[i]);
+        __syncwarp();
+        int32_t* orow = out.idx + qi * (int64_t)k;
+        for (int i = lane; i < n2; i += 32) {
+          const uint32_t ki = s.key[i], oi = s.id[i];
+          int rank = 0;
+          for (int j = 0; j < n2; ++j) {
+            const uint32_t kj = s.key[j], oj = s.id[j];
+            rank += (kj > ki) || (kj == ki && oj > oi);
+          }
+          orow[rank] = (int32_t)oi;
+        }
+        for (int r = n2 + lane; r < k; r += 32) orow[r] = -1;
+        if (lane == 0) {
+          out.count[qi] = n2;
+          out.maxd2[qi] = maxd2;
+        }
+      }
+      __syncwarp();
+
+      if (!bad && kept >= k) {
+        have_prev = true;
+        pqx = qx; pqy = qy; pqz = qz;
+        pkth = maxd2;
+      } else {
+        have_prev = false;
+      }
+    }
+  }
+}
+
+template <int C, int MODE>
+static cudaError_t launch_one(const MapDev& m, const void* queries,
+                              int64_t nq, int k, float n_emitted, KnnOut out,
+                              unsigned long long* counter, int num_sms,
+                              cudaStream_t st) {
+  constexpr int kThreads = (C <= 512) ? 256 : 128;
+  const size_t smem = (kThreads / 32) * sizeof(WarpBuf<C>);
+  auto kern = knn_kernel<C, MODE>;
+  cudaError_t e = cudaFuncSetAttribute(
+      kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kThreads,
+                                                    smem);
+  if (e != cudaSuccess) return e;
+  if (per_sm < 1) per_sm = 1;
+  const int64_t chunks = (nq + kChunk - 1) / kChunk;
+  const int64_t warps_per_block = kThreads / 32;
+  int64_t blocks = (int64_t)num_sms * per_sm;
+  const int64_t need = (chunks + warps_per_block - 1) / warps_per_block;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  kern<<<(unsigned)blocks, kThreads, smem, st>>>(m, queries, nq, k, n_emitted,
+                                                 out, counter);
+  return cudaGetLastError();
+}
+
+cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
+                       int k, int mode, float n_emitted, KnnOut out,
+                       unsigned long long* counter, int num_sms,
+                       cudaStream_t st) {
+  if (nq <= 0) return cudaSuccess;
+  if (k <= 256) {
+    return mode == kModeRadiance
+               ? launch_one<512, kModeRadiance>(m, queries, nq, k, n_emitted,
+                                                out, counter, num_sms, st)
+               : launch_one<512, kModeKnn>(m, queries, nq, k, n_emitted, out,
+                                           counter, num_sms, st);
+  }
+  return mode == kModeRadiance
+             ? launch_one<2048, kModeRadiance>(m, queries, nq, k, n_emitted,
+                                               out, counter, num_sms, st)
+             : launch_one<2048, kModeKnn>(m, queries, nq, k, n_emitted, out,
+                                          counter, num_sms, st);
+}
+
+}  // namespace pm

@@ -1,0 +1,66 @@
+// Device photon map: layout and the launch functions of its kernels.
+//
+// Layout in HBM (n photons):
+//   aos    float[9n]   photons in index order, {throughput, position, wi}
+//                      (the Photon record of photon_map.h:10-22), kept for
+//                      getIthPhoton and for rebuilding.
+//   pos4   float4[n]   sorted by 30-bit Morton code of the position, ties by
+//                      index: {x, y, z, index bits}. The kNN scan reads only
+//                      this array (16 B per photon, one coalesced 512 B
+//                      line per 32-photon leaf).
+//   thr4   float4[n]   same order: {throughput.rgb, wi.x}
+//   wi2    float2[n]   same order: {wi.y, wi.z}
+//   boxes  float4[2m]  32-ary box tree over the sorted array: level 0 has
+//                      one box per 32-photon leaf, level l+1 one box per 32
+//                      level-l boxes; node j of all levels is {lo, hi} at
+//                      boxes[2j], boxes[2j+1].
+#pragma once
+
+#include "pm_common.cuh"
+
+namespace pm {
+
+constexpr int kMaxLevels = 8;
+
+struct MapDev {
+  const float4* __restrict__ pos4;
+  const float4* __restrict__ thr4;
+  const float2* __restrict__ wi2;
+  const float4* __restrict__ boxes;
+  int n;
+  int nlevels;
+  int lvl_off[kMaxLevels];
+  int lvl_cnt[kMaxLevels];
+};
+
+// Tree shape for n photons (host side). Returns the total number of boxes.
+int map_levels(int64_t n, int* nlevels, int* lvl_off, int* lvl_cnt);
+
+// Bytes of scratch the build needs for n photons.
+size_t map_build_scratch_bytes(int64_t n);
+
+// Builds pos4/thr4/wi2/boxes from `aos` (device, 9 floats per photon).
+void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
+                      float2* wi2, float4* boxes, const int* lvl_off,
+                      const int* lvl_cnt, int nlevels, void* scratch,
+                      cudaStream_t st);
+
+enum KnnMode { kModeRadiance = 0, kModeKnn = 1 };
+
+struct KnnOut {
+  float* rgb;          // radiance mode: 3 floats per query
+  int32_t* idx;        // knn mode: k per query
+  int32_t* count;      // knn mode
+  float* maxd2;        // knn mode
+};
+
+// Launches the warp-per-query k-nearest-neighbour kernel.
+//   radiance mode: queries = pm_radiance_query records (3 float4 each)
+//   knn mode:      queries = 3 floats per query
+// `counter` is one device word of scratch (reset by this call).
+cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
+                       int k, int mode, float n_emitted, KnnOut out,
+                       unsigned long long* counter, int num_sms,
+                       cudaStream_t st);
+
+}  // namespace pm

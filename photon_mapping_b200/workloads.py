@@ -1,0 +1,191 @@
+"""Seeded synthetic photon sets and query sets.
+
+These stand in for photon maps and hit points when a test or benchmark
+needs one without tracing a scene: uniform photons in the unit cube,
+photons lying on the five walls of the [0,1]^3 Cornell room (the layout a
+traced photon map has: points on surfaces, directions in the hemisphere
+above each surface), and lattice photons that make many distances tie.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+# The five walls of the unit Cornell room: (axis, value, inward normal, albedo)
+WALLS = (
+    (1, 0.0, (0.0, 1.0, 0.0), (0.73, 0.73, 0.73)),      # floor
+    (1, 1.0, (0.0, -1.0, 0.0), (0.73, 0.73, 0.73)),     # ceiling
+    (2, 0.0, (0.0, 0.0, 1.0), (0.73, 0.73, 0.73)),      # back wall
+    (0, 0.0, (1.0, 0.0, 0.0), (0.63, 0.065, 0.05)),     # left wall (red)
+    (0, 1.0, (-1.0, 0.0, 0.0), (0.14, 0.45, 0.09)),     # right wall (green)
+)
+
+
+def _unit(v: np.ndarray) -> np.ndarray:
+    return v / np.linalg.norm(v, axis=-1, keepdims=True)
+
+
+def hemisphere(rng: np.random.Generator, normals: np.ndarray) -> np.ndarray:
+    """Uniform unit directions with dot(d, n) > 0 for each row of normals."""
+    d = _unit(rng.normal(size=normals.shape))
+    flip = np.sum(d * normals, axis=1) < 0
+    d[flip] = -d[flip]
+    return d
+
+
+def uniform_photons(n: int, seed: int = 0) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    ph = np.empty((n, 9), np.float32)
+    ph[:, 0:3] = rng.uniform(0.0, 2.0, size=(n, 3))
+    ph[:, 3:6] = rng.uniform(0.0, 1.0, size=(n, 3))
+    ph[:, 6:9] = _unit(rng.normal(size=(n, 3)))
+    return ph
+
+
+def wall_points(rng: np.random.Generator, n: int):
+    """n points on the Cornell walls: (positions, inward normals, albedos)."""
+    w = rng.integers(0, len(WALLS), size=n)
+    pos = rng.uniform(0.0, 1.0, size=(n, 3))
+    nrm = np.empty((n, 3))
+    rho = np.empty((n, 3))
+    for i, (axis, val, nn, alb) in enumerate(WALLS):
+        m = w == i
+        pos[m, axis] = val
+        nrm[m] = nn
+        rho[m] = alb
+    return pos, nrm, rho
+
+
+def wall_photons(n: int, seed: int = 0) -> np.ndarray:
+    """Photons on the walls with wi in the hemisphere above the wall."""
+    rng = np.random.default_rng(seed)
+    pos, nrm, rho = wall_points(rng, n)
+    ph = np.empty((n, 9), np.float32)
+    ph[:, 0:3] = rng.uniform(0.0, 1.5, size=(n, 3)) * rho
+    ph[:, 3:6] = pos
+    ph[:, 6:9] = hemisphere(rng, nrm)
+    # a few photons arriving from below the surface (grazing leaks) so the
+    # Lambert cosine test has both outcomes
+    leak = rng.random(n) < 0.05
+    ph[leak, 6:9] = -ph[leak, 6:9]
+    return ph
+
+
+def lattice_photons(m: int = 12, spacing: float = 0.125, seed: int = 0) -> np.ndarray:
+    """Photons on an m^3 lattice: many exactly equal distances."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(m, dtype=np.float32) * np.float32(spacing)
+    x, y, z = np.meshgrid(g, g, g, indexing="ij")
+    n = m ** 3
+    ph = np.empty((n, 9), np.float32)
+    ph[:, 0:3] = rng.uniform(0.1, 1.0, size=(n, 3))
+    ph[:, 3] = x.ravel()
+    ph[:, 4] = y.ravel()
+    ph[:, 5] = z.ravel()
+    ph[:, 6:9] = _unit(rng.normal(size=(n, 3)))
+    return ph
+
+
+def wall_queries(n: int, seed: int = 1) -> np.ndarray:
+    """pm_radiance_query records (n, 12) for points on the walls: wo in the
+    hemisphere above the wall, ns = the wall normal, rho = its albedo."""
+    rng = np.random.default_rng(seed)
+    pos, nrm, rho = wall_points(rng, n)
+    wo = hemisphere(rng, nrm)
+    q = np.empty((n, 12), np.float32)
+    q[:, 0:3], q[:, 3] = pos, rho[:, 0]
+    q[:, 4:7], q[:, 7] = wo, rho[:, 1]
+    q[:, 8:11], q[:, 11] = nrm, rho[:, 2]
+    return q
+
+
+# --------------------------------------------------------------- camera rays
+
+_PCG_MULT = np.uint64(6364136223846793005)
+
+
+def pcg32_next(state: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """One PCG32 XSH-RR step for many generators with inc = 1, as the
+    reference's RNG (sampler.h:11-47): returns (uint32 output, new state)."""
+    old = state
+    with np.errstate(over="ignore"):
+        new = old * _PCG_MULT + np.uint64(1)
+    xs = (((old >> np.uint64(18)) ^ old) >> np.uint64(27)).astype(np.uint32)
+    rot = (old >> np.uint64(59)).astype(np.uint32)
+    out = (xs >> rot) | (xs << ((np.uint32(32) - rot) & np.uint32(31)))
+    return out.astype(np.uint32), new
+
+
+def pcg32_float(u: np.ndarray) -> np.ndarray:
+    """RNG::getNext: float(u32) * (1.0f / UINT32_MAX) in float32 (1.0 reachable)."""
+    return u.astype(np.float32) * np.float32(1.0 / 4294967295.0)
+
+
+ROOM_CAMERA = dict(position=(0.5, 0.5, 4.7), forward=(0.0, 0.0, -1.0), fov=0.25 * 3.14159265359)
+LIGHT_MIN, LIGHT_MAX, LIGHT_Y = 0.375, 0.625, 0.999
+
+
+def room_primary_hit_queries(width: int = 512, height: int = 512, spp: int = 4) -> np.ndarray:
+    """pm_radiance_query records for the primary hits of a width x height x spp
+    frame of the empty unit Cornell room (five walls, ceiling light quad).
+
+    Camera samples follow the reference's render loop (examples/main.cpp:33-47
+    with camera.h:41-47): pixel (i, j) owns a sampler seeded j + width*i and
+    each sample draws the u then the v jitter; with no final gathering a
+    diffuse hit draws nothing else, so sample s uses draws 2s and 2s+1.
+    Queries come in pixel-major, sample-minor order; rays that hit the light
+    (which returns Le, no photon-map query) are left out.
+    """
+    f32 = np.float32
+    pos = np.array(ROOM_CAMERA["position"], f32)
+    fwd = np.array(ROOM_CAMERA["forward"], f32)
+    right = np.cross(fwd, np.array([0, 1, 0], f32)).astype(f32)
+    right = right / np.sqrt(f32(np.dot(right, right)))
+    up = np.cross(right, fwd).astype(f32)
+    up = up / np.sqrt(f32(np.dot(up, up)))
+    focal = f32(1.0) / f32(np.tan(f32(0.5) * f32(ROOM_CAMERA["fov"])))
+    ii, jj = np.meshgrid(np.arange(height), np.arange(width), indexing="ij")
+    state = (jj + width * ii).astype(np.uint64).ravel()
+    jf = jj.ravel().astype(f32)
+    if_ = ii.ravel().astype(f32)
+    rays_o, rays_d = [], []
+    for _ in range(spp):
+        a, state = pcg32_next(state)
+        b, state = pcg32_next(state)
+        u = (f32(2.0) * (jf + pcg32_float(a)) - f32(width)) / f32(height)
+        v = (f32(2.0) * (if_ + pcg32_float(b)) - f32(height)) / f32(height)
+        pin = pos + focal * fwd
+        sensor = pos[None, :] + u[:, None] * right[None, :] + v[:, None] * up[None, :]
+        d = (pin[None, :] - sensor).astype(f32)
+        d = d / np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])[:, None]
+        rays_o.append(sensor)
+        rays_d.append(d)
+    o = np.stack(rays_o, axis=1).reshape(-1, 3).astype(np.float64)
+    d = np.stack(rays_d, axis=1).reshape(-1, 3).astype(np.float64)
+    best_t = np.full(o.shape[0], np.inf)
+    best_w = np.full(o.shape[0], -1)
+    for wi, (axis, val, nn, alb) in enumerate(WALLS):
+        with np.errstate(divide="ignore", invalid="ignore"):
+            t = (val - o[:, axis]) / d[:, axis]
+        p = o + t[:, None] * d
+        inside = np.ones(o.shape[0], bool)
+        for ax in range(3):
+            if ax != axis:
+                inside &= (p[:, ax] >= 0.0) & (p[:, ax] <= 1.0)
+        ok = inside & (t > 1e-5) & (t < best_t)
+        best_t[ok] = t[ok]
+        best_w[ok] = wi
+    with np.errstate(divide="ignore", invalid="ignore"):
+        tl = (LIGHT_Y - o[:, 1]) / d[:, 1]
+    pl = o + tl[:, None] * d
+    light = ((tl > 1e-5) & (tl < best_t) & (pl[:, 0] >= LIGHT_MIN) & (pl[:, 0] <= LIGHT_MAX)
+             & (pl[:, 2] >= LIGHT_MIN) & (pl[:, 2] <= LIGHT_MAX))
+    keep = (best_w >= 0) & ~light
+    hit = o[keep] + best_t[keep, None] * d[keep]
+    w = best_w[keep]
+    nrm = np.array([WALLS[i][2] for i in range(len(WALLS))])[w]
+    rho = np.array([WALLS[i][3] for i in range(len(WALLS))])[w]
+    q = np.empty((hit.shape[0], 12), np.float32)
+    q[:, 0:3], q[:, 3] = hit, rho[:, 0]
+    q[:, 4:7], q[:, 7] = -d[keep], rho[:, 1]
+    q[:, 8:11], q[:, 11] = nrm, rho[:, 2]
+    return q
