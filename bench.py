@@ -46,7 +46,7 @@ CPU_SAMPLE_QUERIES = 40000
 def parse_args():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -212,7 +212,8 @@ def run_ours(args) -> None:
     d_q = torch.from_numpy(queries).to(dev)
     d_out = torch.empty((nq, 3), dtype=torch.float32, device=dev)
     flush = torch.empty(64 << 20, dtype=torch.float32, device=dev)  # 256 MiB > L2
-    stream = torch.cuda.current_stream(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
 
     def step():
         st = lib.pm_photonmap_radiance_device(ctx.handle, 0, d_q.data_ptr(), nq, K_NEAREST,
@@ -241,7 +242,6 @@ def run_ours(args) -> None:
     t_wall = time.perf_counter() - t_wall
     if dist:
         dist.barrier()
-    clk = clocks.stop()
     times = [e0.elapsed_time(e1) for e0, e1 in evs]
     ms = sum(times) / len(times)
     if dist:
@@ -276,6 +276,15 @@ def run_ours(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     e2e_value = world * nq / e2e_s
+    clk = clocks.stop()  # sampled over the timed steps and the e2e steps
+
+    # one more (untimed) pass with the kernel's counters on
+    ctx.set_stats(True)
+    step()
+    torch.cuda.synchronize(dev)
+    st = ctx.get_stats(reset=True)
+    ctx.set_stats(False)
+    per_q = {k2: v / max(st["queries"], 1) for k2, v in st.items() if k2 != "queries"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -313,6 +322,7 @@ def run_ours(args) -> None:
                 "h2d_bytes_per_step": int(queries.nbytes),
                 "d2h_bytes_per_step": int(nq * 3 * 4)},
         "gpu_launches": args.steps,
+        "knn_per_query": per_q,
         "clocks": clk,
         "wall_s_timed_region": t_wall,
     }

@@ -10,8 +10,9 @@
  *     across this boundary. pm_ctx_last_error() gives a message for the last
  *     failing call on a context.
  *   - Host pointers are copied before the call returns ("host" API). The
- *     *_device variants take device pointers and a cudaStream_t (as void*),
- *     enqueue asynchronously on that stream and return immediately.
+ *     *_device variants take device pointers and a cudaStream_t (as void*;
+ *     NULL is CUDA's legacy default stream), enqueue asynchronously on that
+ *     stream and return immediately.
  *   - All device allocations are owned by the context and released by
  *     pm_ctx_destroy(). Calls on one context are serialised by a mutex, so a
  *     context may be shared by host threads (the reference calls integrate()
@@ -70,12 +71,30 @@ const char* pm_ctx_last_error(const pm_ctx* ctx);
 /* Static name of a status code. */
 const char* pm_status_string(int status);
 
+/* Counters of the k-nearest-neighbour kernels (diagnostics; no reference
+ * counterpart). Collected only while enabled with pm_ctx_set_stats. */
+typedef struct pm_knn_stats {
+  uint64_t queries;     /* queries answered                                  */
+  uint64_t cold_starts; /* queries whose search radius was bounded afresh    */
+  uint64_t candidates;  /* photons found within the search radius            */
+  uint64_t leaves;      /* 8-photon groups scanned                           */
+  uint64_t nodes;       /* inner tree nodes expanded                         */
+  uint64_t selects;     /* k-th distance selections                          */
+} pm_knn_stats;
+
+/* Turns the kNN counters on (1) or off (0) for later launches. */
+int pm_ctx_set_stats(pm_ctx* ctx, int enable);
+/* Copies the counters (waits for the context's stream); reset != 0 zeroes
+ * them afterwards. */
+int pm_ctx_get_stats(pm_ctx* ctx, pm_knn_stats* out, int reset);
+
 /* ---------------------------------------------------------- photon map */
 /* Replaces PhotonMap::setPhotons + PhotonMap::build
  * (photon_map.h:198-206, KdTree::buildTree photon_map.h:157-164).
  * `photons` holds n records of 9 floats (see above); n == 0 gives an empty
  * map, which every query answers with no neighbours. The map is rebuilt on
- * the device: Morton codes, radix sort, 32-photon leaves, 32-ary box tree. */
+ * the device: Morton codes, radix sort, boxes over 8-photon groups, 32-ary
+ * box tree above them. */
 int pm_photonmap_build(pm_ctx* ctx, int map, const float* photons, int64_t n);
 
 /* Same as pm_photonmap_build with `d_photons` in device memory. */

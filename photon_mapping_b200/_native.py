@@ -48,6 +48,8 @@ _SIGNATURES = {
     "pm_ctx_synchronize": (C.c_int, [_vp]),
     "pm_ctx_last_error": (C.c_char_p, [_vp]),
     "pm_status_string": (C.c_char_p, [C.c_int]),
+    "pm_ctx_set_stats": (C.c_int, [_vp, C.c_int]),
+    "pm_ctx_get_stats": (C.c_int, [_vp, _vp, C.c_int]),
     "pm_photonmap_build": (C.c_int, [_vp, C.c_int, _vp, _i64]),
     "pm_photonmap_build_device": (C.c_int, [_vp, C.c_int, _vp, _i64, _vp]),
     "pm_photonmap_size": (C.c_int, [_vp, C.c_int, C.POINTER(_i64)]),
@@ -130,3 +132,14 @@ class Context:
 
     def synchronize(self) -> None:
         self.check(self.lib.pm_ctx_synchronize(self.handle), "synchronize")
+
+    STAT_FIELDS = ("queries", "cold_starts", "candidates", "leaves", "nodes", "selects")
+
+    def set_stats(self, enable: bool) -> None:
+        self.check(self.lib.pm_ctx_set_stats(self.handle, int(bool(enable))), "pm_ctx_set_stats")
+
+    def get_stats(self, reset: bool = False) -> dict:
+        buf = (C.c_uint64 * len(self.STAT_FIELDS))()
+        self.check(self.lib.pm_ctx_get_stats(self.handle, C.addressof(buf), int(reset)),
+                   "pm_ctx_get_stats")
+        return dict(zip(self.STAT_FIELDS, (int(v) for v in buf)))

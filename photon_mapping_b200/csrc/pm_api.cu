@@ -110,9 +110,9 @@ int build_map(pm_ctx* c, DevMap& dm, const float* d_aos, int64_t n,
 
 }  // namespace pm
 
-static inline cudaStream_t as_stream(pm_ctx* c, void* s) {
-  return s ? (cudaStream_t)s : c->stream;
-}
+// Streams passed through the C ABI follow CUDA's convention: NULL is the
+// legacy default stream.
+static inline cudaStream_t as_stream(void* s) { return (cudaStream_t)s; }
 
 #define PM_CHECK_CTX(c)                                   \
   do {                                                    \
@@ -189,6 +189,35 @@ int pm_ctx_synchronize(pm_ctx* c) {
   return cuda_status(c, cudaStreamSynchronize(c->stream), "synchronize");
 }
 
+int pm_ctx_set_stats(pm_ctx* c, int enable) {
+  PM_CHECK_CTX(c);
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (enable && !c->stats.ptr) {
+    int s = c->stats.ensure(8 * sizeof(unsigned long long));
+    if (s != PM_OK) return set_err(c, s, "stats counters");
+    cudaError_t e = cudaMemsetAsync(c->stats.ptr, 0, c->stats.bytes, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) return cuda_status(c, e, "stats counters");
+  }
+  c->stats_on = enable != 0;
+  return PM_OK;
+}
+
+int pm_ctx_get_stats(pm_ctx* c, pm_knn_stats* out, int reset) {
+  PM_CHECK_CTX(c);
+  if (!out) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  memset(out, 0, sizeof(*out));
+  if (!c->stats.ptr) return PM_OK;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e == cudaSuccess)
+    e = cudaMemcpy(out, c->stats.ptr, sizeof(*out), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && reset) e = cudaMemset(c->stats.ptr, 0, c->stats.bytes);
+  return cuda_status(c, e, "stats read");
+}
+
 const char* pm_ctx_last_error(const pm_ctx* c) {
   return c ? c->err.c_str() : "null context";
 }
@@ -224,7 +253,7 @@ int pm_photonmap_build_device(pm_ctx* c, int map, const void* d_photons,
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
   return build_map(c, c->maps[map], (const float*)d_photons, n,
-                   as_stream(c, stream));
+                   as_stream(stream));
 }
 
 int pm_photonmap_size(pm_ctx* c, int map, int64_t* n) {
@@ -284,6 +313,7 @@ int pm_photonmap_knn(pm_ctx* c, int map, const float* queries, int64_t nq,
       cudaMemcpyAsync(c->q_in.ptr, queries, qb, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return cuda_status(c, e, "query upload");
   KnnOut o{};
+  o.stats = c->stats_ptr();
   o.idx = (int32_t*)c->q_out.ptr;
   o.count = (int32_t*)((char*)c->q_out.ptr + ib);
   o.maxd2 = (float*)((char*)c->q_out.ptr + ib + cb);
@@ -324,6 +354,7 @@ int pm_photonmap_radiance(pm_ctx* c, int map, const pm_radiance_query* q,
                                   st);
   if (e != cudaSuccess) return cuda_status(c, e, "query upload");
   KnnOut o{};
+  o.stats = c->stats_ptr();
   o.rgb = (float*)c->q_out.ptr;
   e = knn_launch(map_view(dm), c->q_in.ptr, nq, k, kModeRadiance,
                  (float)n_emitted, o, c->next_counter(), c->num_sms, st);
@@ -351,10 +382,11 @@ int pm_photonmap_radiance_device(pm_ctx* c, int map, const void* d_queries,
   DevMap& dm = c->maps[map];
   if (!dm.built) return set_err(c, PM_ERR_NOT_BUILT, "map %d not built", map);
   KnnOut o{};
+  o.stats = c->stats_ptr();
   o.rgb = (float*)d_out_rgb;
   cudaError_t e = knn_launch(map_view(dm), d_queries, nq, k, kModeRadiance,
                              (float)n_emitted, o, c->next_counter(),
-                             c->num_sms, as_stream(c, stream));
+                             c->num_sms, as_stream(stream));
   return cuda_status(c, e, "radiance launch");
 }
 

@@ -54,6 +54,11 @@ struct pm_ctx {
   pm::DevBuf q_in, q_out;  // staging of the host-pointer entry points
   pm::DevBuf counter;      // kCounterRing work counters
   unsigned counter_next = 0;
+  pm::DevBuf stats;        // pm_knn_stats counters (device)
+  bool stats_on = false;
+  unsigned long long* stats_ptr() {
+    return stats_on ? (unsigned long long*)stats.ptr : nullptr;
+  }
 
   unsigned long long* next_counter() {
     unsigned long long* base = (unsigned long long*)counter.ptr;
@@ -66,6 +71,7 @@ struct pm_ctx {
     q_in.release();
     q_out.release();
     counter.release();
+    stats.release();
   }
 };
 

@@ -24,7 +24,7 @@ int map_levels(int64_t n, int* nlevels, int* lvl_off, int* lvl_cnt) {
     *nlevels = 0;
     return 0;
   }
-  int64_t cnt = (n + 31) / 32;
+  int64_t cnt = (n + kGroup - 1) / kGroup;
   int lv = 0, off = 0;
   while (true) {
     lvl_off[lv] = off;
@@ -132,21 +132,21 @@ __global__ void gather_kernel(const float* __restrict__ aos, int n,
   wi2[s] = make_float2(r[7], r[8]);
 }
 
-__global__ void leaf_box_kernel(const float4* __restrict__ pos4, int n,
-                                int nleaves, float4* __restrict__ boxes) {
-  const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const int lane = threadIdx.x & 31;
-  if (warp >= nleaves) return;
-  const int i = warp * 32 + lane;
+// Box of each 8-photon group: 8 lanes per group, 4 groups per warp.
+__global__ void group_box_kernel(const float4* __restrict__ pos4, int n,
+                                 int ngroups, float4* __restrict__ boxes) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int g = t >> 3;
+  const int i = g * kGroup + (threadIdx.x & 7);
   float4 lo = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, 0.f);
   float4 hi = make_float4(-FLT_MAX, -FLT_MAX, -FLT_MAX, 0.f);
-  if (i < n) {
+  if (g < ngroups && i < n) {
     const float4 p = pos4[i];
     lo.x = fminf(lo.x, p.x); lo.y = fminf(lo.y, p.y); lo.z = fminf(lo.z, p.z);
     hi.x = fmaxf(hi.x, p.x); hi.y = fmaxf(hi.y, p.y); hi.z = fmaxf(hi.z, p.z);
   }
 #pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
+  for (int o = 4; o > 0; o >>= 1) {
     lo.x = fminf(lo.x, __shfl_xor_sync(kFull, lo.x, o));
     lo.y = fminf(lo.y, __shfl_xor_sync(kFull, lo.y, o));
     lo.z = fminf(lo.z, __shfl_xor_sync(kFull, lo.z, o));
@@ -154,9 +154,9 @@ __global__ void leaf_box_kernel(const float4* __restrict__ pos4, int n,
     hi.y = fmaxf(hi.y, __shfl_xor_sync(kFull, hi.y, o));
     hi.z = fmaxf(hi.z, __shfl_xor_sync(kFull, hi.z, o));
   }
-  if (lane == 0) {
-    boxes[2 * warp] = lo;
-    boxes[2 * warp + 1] = hi;
+  if (g < ngroups && (threadIdx.x & 7) == 0) {
+    boxes[2 * g] = lo;
+    boxes[2 * g + 1] = hi;
   }
 }
 
@@ -208,9 +208,9 @@ void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
   morton_kernel<<<gb, tb, 0, st>>>(aos, n, bb, ka, va);
   const bool in_b = radix_sort_pairs<uint32_t>(ka, va, kb, vb, n, 30, hist, st);
   gather_kernel<<<gb, tb, 0, st>>>(aos, n, in_b ? vb : va, pos4, thr4, wi2);
-  const int nleaves = lvl_cnt[0];
-  leaf_box_kernel<<<(nleaves * 32 + tb - 1) / tb, tb, 0, st>>>(pos4, n, nleaves,
-                                                               boxes);
+  const int ngroups = lvl_cnt[0];
+  group_box_kernel<<<(int)(((int64_t)ngroups * kGroup + tb - 1) / tb), tb, 0,
+                     st>>>(pos4, n, ngroups, boxes);
   for (int l = 1; l < nlevels; ++l) {
     node_box_kernel<<<(lvl_cnt[l] * 32 + tb - 1) / tb, tb, 0, st>>>(
         boxes, lvl_off[l - 1], lvl_cnt[l - 1], lvl_off[l], lvl_cnt[l]);
@@ -218,9 +218,23 @@ void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
 }
 
 // -------------------------------------------------------------- kNN query
+//
+// One warp answers one query at a time, walking a chunk of consecutive
+// queries. Per query:
+//   1. bound: an upper bound tau of the k-th distance. From the previous
+//      query of the chunk by the triangle inequality when it is close
+//      ((r_prev + delta)^2, inflated for rounding), else from the photons
+//      Morton-adjacent to the group nearest the query.
+//   2. collect: depth-first walk of the 32-ary box tree; the passing
+//      8-photon groups of a node are scanned packed, 4 groups per round,
+//      every photon with dist2 <= tau appended to the warp's buffer. A
+//      nearly full buffer is cut to the k best, lowering tau.
+//   3. select: radix select of the exact k-th (dist2, index) pair.
+//   4. output: the radiance sum (Lambert, integrator.h:141-150) or the
+//      index list in the reference's order.
 
-constexpr int kStack = 256;  // 32 entries per tree level, 8 levels
-constexpr int kChunk = 32;   // queries a warp takes per work-counter bump
+constexpr int kStack = 32 * kMaxLevels;
+constexpr int kChunk = 32;  // queries a warp takes per work-counter bump
 
 template <int C>
 struct WarpBuf {
@@ -228,10 +242,27 @@ struct WarpBuf {
   uint32_t id[C];   // sorted position of the photon
   uint32_t hist[256];
   uint32_t stack[kStack];
+  uint32_t list[32];  // passing groups of the node being scanned
+  uint32_t sel[32];   // entries of the critical bin of a selection
+  uint32_t stat[8];   // per-warp counters, same order as pm_knn_stats
 };
 
-__device__ __forceinline__ uint32_t orig_index(const MapDev& m, uint32_t s) {
-  return __float_as_uint(m.pos4[s].w);
+struct Levels {
+  int off[kMaxLevels];
+  int cnt[kMaxLevels];
+};
+
+enum { kStatQueries = 0, kStatCold, kStatCand, kStatLeaves, kStatNodes, kStatSelects };
+
+// Counters are compiled in only for the kernels launched with statistics.
+template <bool S, int C>
+__device__ __forceinline__ void stat_add(WarpBuf<C>& s, int lane, int which,
+                                         uint32_t v) {
+  if (S && lane == 0) s.stat[which] += v;
+}
+
+__device__ __forceinline__ uint32_t orig_index(const float4* pos4, uint32_t s) {
+  return __float_as_uint(pos4[s].w);
 }
 
 // k-th smallest (1-based) value among the valid entries i in [0, cnt),
@@ -322,13 +353,124 @@ __device__ uint32_t warp_select(uint32_t* hist, int cnt, uint32_t kk, Get get,
   return prefix;
 }
 
+// Finds the bin holding the kk-th smallest entry of a 256-bin histogram
+// already filled (sum >= kk): returns the bin; *kk_in = rank inside it
+// (1-based), *n_bin = entries in it.
+__device__ __forceinline__ uint32_t hist_find(const uint32_t* hist, uint32_t kk,
+                                              int lane, uint32_t* kk_in,
+                                              uint32_t* n_bin) {
+  uint32_t h[8];
+  uint32_t sum = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    h[j] = hist[lane * 8 + j];
+    sum += h[j];
+  }
+  uint32_t incl = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t t = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += t;
+  }
+  const uint32_t excl = incl - sum;
+  const unsigned owner = __ballot_sync(kFull, excl < kk && kk <= incl);
+  const int ol = __ffs(owner) - 1;
+  uint32_t bin = 0, nk = 0, cd = 0;
+  if (lane == ol) {
+    uint32_t run = excl;
+    bool found = false;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      if (!found) {
+        if (run + h[j] >= kk) {
+          bin = (uint32_t)(lane * 8 + j);
+          nk = kk - run;
+          cd = h[j];
+          found = true;
+        } else {
+          run += h[j];
+        }
+      }
+    }
+  }
+  *kk_in = __shfl_sync(kFull, nk, ol);
+  *n_bin = __shfl_sync(kFull, cd, ol);
+  return __shfl_sync(kFull, bin, ol);
+}
+
+// Fast exact selection for a buffer whose dist2 all lie in [0, tau]:
+// one histogram of dist2 over 256 equal bins of [0, tau] (bin = floor(d2 *
+// 256/tau) is monotone in d2, so every entry of a lower bin is smaller),
+// then the critical bin is ranked exactly by (dist2, index) across lanes.
+// Photons on surfaces give dist2 close to uniform on [0, tau], so the
+// critical bin holds one or two entries. Returns false (caller falls back
+// to the radix select) when tau is not a positive finite bound or the
+// critical bin holds more than 32 entries.
+template <int C>
+__device__ __forceinline__ bool select_kth_hist(const float4* pos4,
+                                                WarpBuf<C>& s, int cnt, int k,
+                                                float tau, int lane,
+                                                uint32_t& kth_key,
+                                                uint32_t& kth_oid) {
+  const float sc = __fdiv_rn(256.f, tau);
+  if (!(tau > 0.f) || !(sc < __int_as_float(0x7f800000))) return false;
+  for (int b = lane; b < 256; b += 32) s.hist[b] = 0;
+  __syncwarp();
+  for (int i = lane; i < cnt; i += 32) {
+    const float d2 = __uint_as_float(s.key[i]);
+    const int b = min(255, __float2int_rz(__fmul_rz(d2, sc)));
+    atomicAdd(&s.hist[b], 1u);
+  }
+  __syncwarp();
+  uint32_t kk, nb;
+  const int bin = (int)hist_find(s.hist, (uint32_t)k, lane, &kk, &nb);
+  if (nb > 32) return false;
+  int pos = 0;
+  for (int base = 0; base < cnt; base += 32) {
+    const int i = base + lane;
+    bool in = false;
+    if (i < cnt)
+      in = min(255, __float2int_rz(__fmul_rz(__uint_as_float(s.key[i]), sc))) ==
+           bin;
+    const unsigned bal = __ballot_sync(kFull, in);
+    if (in) s.sel[pos + __popc(bal & lanemask_lt())] = (uint32_t)i;
+    pos += __popc(bal);
+  }
+  __syncwarp();
+  uint32_t kj = 0xffffffffu, oj = 0xffffffffu;
+  if (lane < (int)nb) {
+    const uint32_t i = s.sel[lane];
+    kj = s.key[i];
+    oj = orig_index(pos4, s.id[i]);
+  }
+  int rank = 0;
+  for (int t = 0; t < (int)nb; ++t) {
+    const uint32_t kt = __shfl_sync(kFull, kj, t);
+    const uint32_t ot = __shfl_sync(kFull, oj, t);
+    rank += (kt < kj) || (kt == kj && ot < oj);
+  }
+  const unsigned who = __ballot_sync(kFull, lane < (int)nb && rank == (int)kk - 1);
+  const int wl = __ffs(who) - 1;
+  kth_key = __shfl_sync(kFull, kj, wl);
+  kth_oid = __shfl_sync(kFull, oj, wl);
+  // a key held by one entry only: keep every entry with that key
+  const unsigned same = __ballot_sync(kFull, lane < (int)nb && kj == kth_key);
+  if (__popc(same) == 1) kth_oid = 0xffffffffu;
+  __syncwarp();
+  return true;
+}
+
 // Exact k-th smallest (dist2, index) pair of the buffer: kth_key, and
 // kth_oid = largest original index kept among entries with key == kth_key
-// (0xffffffff when all of them are kept).
-template <int C>
-__device__ void select_kth(const MapDev& m, WarpBuf<C>& s, int cnt, int k,
-                           int lane, uint32_t& kth_key, uint32_t& kth_oid) {
+// (0xffffffff when all of them are kept). Every entry has dist2 <= tau.
+template <int C, bool S>
+__device__ __forceinline__ void select_kth(const float4* pos4, WarpBuf<C>& s,
+                                           int cnt, int k, float tau, int lane,
+                                           uint32_t& kth_key,
+                                           uint32_t& kth_oid) {
   uint32_t rank_eq, n_eq;
+  stat_add<S>(s, lane, kStatSelects, 1);
+  if (select_kth_hist(pos4, s, cnt, k, tau, lane, kth_key, kth_oid)) return;
   kth_key = warp_select(
       s.hist, cnt, (uint32_t)k,
       [&](int i, uint32_t& v) {
@@ -344,31 +486,32 @@ __device__ void select_kth(const MapDev& m, WarpBuf<C>& s, int cnt, int k,
         s.hist, cnt, rank_eq,
         [&](int i, uint32_t& v) {
           if (s.key[i] != kk) return false;
-          v = orig_index(m, s.id[i]);
+          v = orig_index(pos4, s.id[i]);
           return true;
         },
         lane, &r2, &n2);
   }
 }
 
-__device__ __forceinline__ bool keep_entry(const MapDev& m, uint32_t key,
+__device__ __forceinline__ bool keep_entry(const float4* pos4, uint32_t key,
                                            uint32_t id, uint32_t kth_key,
                                            uint32_t kth_oid) {
   if (key < kth_key) return true;
   if (key != kth_key) return false;
-  return kth_oid == 0xffffffffu || orig_index(m, id) <= kth_oid;
+  return kth_oid == 0xffffffffu || orig_index(pos4, id) <= kth_oid;
 }
 
 template <int C>
-__device__ int compact_kept(const MapDev& m, WarpBuf<C>& s, int cnt,
-                            uint32_t kth_key, uint32_t kth_oid, int lane) {
+__device__ __forceinline__ int compact_kept(const float4* pos4, WarpBuf<C>& s,
+                                            int cnt, uint32_t kth_key,
+                                            uint32_t kth_oid, int lane) {
   int dst = 0;
   for (int b = 0; b < cnt; b += 32) {
     const int i = b + lane;
     const bool v = i < cnt;
     const uint32_t key = v ? s.key[i] : 0u;
     const uint32_t id = v ? s.id[i] : 0u;
-    const bool kp = v && keep_entry(m, key, id, kth_key, kth_oid);
+    const bool kp = v && keep_entry(pos4, key, id, kth_key, kth_oid);
     const unsigned bal = __ballot_sync(kFull, kp);
     __syncwarp();
     if (kp) {
@@ -382,42 +525,100 @@ __device__ int compact_kept(const MapDev& m, WarpBuf<C>& s, int cnt,
   return dst;
 }
 
-// Appends every photon of `leaf` with dist2 <= tau. When the buffer is
-// nearly full, keeps only the k best and lowers tau to the k-th distance.
-template <int C>
-__device__ __forceinline__ void scan_leaf(const MapDev& m, int leaf, float qx,
-                                          float qy, float qz, float& tau,
-                                          int& cnt, WarpBuf<C>& s, int lane,
-                                          int k) {
-  const int i = leaf * 32 + lane;
-  const bool ok = i < m.n;
-  float d2 = 0.f;
-  if (ok) {
-    const float4 p = __ldg(m.pos4 + i);
-    d2 = dist2_ref(qx, qy, qz, p.x, p.y, p.z);
-  }
-  const bool pass = ok && d2 <= tau;
+// Per-query state of the search.
+struct Query {
+  float x, y, z;
+  float tau;  // every photon with dist2 <= tau is collected
+  int cnt;    // entries in the warp buffer
+  int k;
+};
+
+// Rare path, kept out of line: the buffer is nearly full. Keeps the k best
+// entries; returns {new count, float bits of the k-th distance}.
+template <int C, bool S>
+__device__ __forceinline__ uint2 tighten(const float4* pos4, WarpBuf<C>* sp,
+                                         int cnt, int k, float tau, int lane) {
+  WarpBuf<C>& s = *sp;
+  uint32_t kth_key, kth_oid;
+  select_kth<C, S>(pos4, s, cnt, k, tau, lane, kth_key, kth_oid);
+  const int n2 = compact_kept(pos4, s, cnt, kth_key, kth_oid, lane);
+  return make_uint2((uint32_t)n2, kth_key);
+}
+
+// Appends photon i (position p) when valid and dist2 <= tau. When the
+// buffer is nearly full, keeps the k best and lowers tau to the k-th.
+template <int C, bool S>
+__device__ __forceinline__ void offer(const MapDev& m, Query& q, WarpBuf<C>& s,
+                                      int lane, const float4& p, int i,
+                                      bool valid) {
+  const float d2 = dist2_ref(q.x, q.y, q.z, p.x, p.y, p.z);
+  const bool pass = valid && d2 <= q.tau;
   const unsigned bal = __ballot_sync(kFull, pass);
   if (pass) {
-    const int o = cnt + __popc(bal & lanemask_lt());
+    const int o = q.cnt + __popc(bal & lanemask_lt());
     s.key[o] = __float_as_uint(d2);
     s.id[o] = (uint32_t)i;
   }
-  cnt += __popc(bal);
-  if (cnt > C - 32) {
+  q.cnt += __popc(bal);
+  if (q.cnt > C - 32) {
     __syncwarp();
-    uint32_t kth_key, kth_oid;
-    select_kth(m, s, cnt, k, lane, kth_key, kth_oid);
-    cnt = compact_kept(m, s, cnt, kth_key, kth_oid, lane);
-    tau = __uint_as_float(kth_key);
+    const uint2 r = tighten<C, S>(m.pos4, &s, q.cnt, q.k, q.tau, lane);
+    q.cnt = (int)r.x;
+    q.tau = __uint_as_float(r.y);
   }
 }
 
-// Depth-first walk of the box tree collecting all photons with dist2 <= tau.
-template <int C>
-__device__ int collect(const MapDev& m, float qx, float qy, float qz,
-                       float& tau, WarpBuf<C>& s, int lane, int k) {
-  int cnt = 0;
+// Scans the photons of the ng groups listed in s.list: lane l handles
+// photon (l & 7) of group 4r + (l >> 3) in round r; two rounds are loaded
+// before either is used.
+template <int C, bool S>
+__device__ __forceinline__ void scan_groups(const MapDev& m, Query& q,
+                                            WarpBuf<C>& s, int lane, int ng) {
+  const int sub = lane >> 3, j = lane & 7;
+  stat_add<S>(s, lane, kStatLeaves, (uint32_t)ng);
+  for (int r = 0; r < ng; r += 8) {
+    const int ga = r + sub, gb = r + 4 + sub;
+    int ia = 0, ib = 0;
+    bool va = ga < ng, vb = gb < ng;
+    if (va) ia = (int)s.list[ga] * kGroup + j;
+    if (vb) ib = (int)s.list[gb] * kGroup + j;
+    va = va && ia < m.n;
+    vb = vb && ib < m.n;
+    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
+    if (va) pa = __ldg(m.pos4 + ia);
+    if (vb) pb = __ldg(m.pos4 + ib);
+    offer<C, S>(m, q, s, lane, pa, ia, va);
+    if (r + 4 < ng) offer<C, S>(m, q, s, lane, pb, ib, vb);
+  }
+  __syncwarp();
+}
+
+// Scans the contiguous photon range [lo, hi), 32 photons per round.
+template <int C, bool S>
+__device__ __forceinline__ void scan_range(const MapDev& m, Query& q,
+                                           WarpBuf<C>& s, int lane, int lo,
+                                           int hi) {
+  for (int b = lo; b < hi; b += 64) {
+    const int ia = b + lane, ib = b + 32 + lane;
+    const bool va = ia < hi, vb = ib < hi;
+    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
+    if (va) pa = __ldg(m.pos4 + ia);
+    if (vb) pb = __ldg(m.pos4 + ib);
+    offer<C, S>(m, q, s, lane, pa, ia, va);
+    if (b + 32 < hi) offer<C, S>(m, q, s, lane, pb, ib, vb);
+  }
+}
+
+// Depth-first walk of the box tree collecting all photons with
+// dist2 <= q.tau into the warp buffer.
+template <int C, bool S>
+__device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
+                                        Query& q, WarpBuf<C>& s, int lane) {
+  q.cnt = 0;
+  if (m.nlevels == 1) {  // a single 8-photon group
+    scan_range<C, S>(m, q, s, lane, 0, m.n);
+    return;
+  }
   const int top = m.nlevels - 1;
   if (lane == 0) s.stack[0] = ((uint32_t)top << 28);
   int sp = 1;
@@ -426,28 +627,22 @@ __device__ int collect(const MapDev& m, float qx, float qy, float qz,
     --sp;
     const uint32_t e = s.stack[sp];
     __syncwarp();
-    const int lvl = (int)(e >> 28);
+    const int cl = (int)(e >> 28) - 1;  // level of the children
     const int node = (int)(e & 0x0fffffffu);
-    if (lvl == 0) {
-      scan_leaf(m, node, qx, qy, qz, tau, cnt, s, lane, k);
-      continue;
-    }
-    const int cl = lvl - 1;
     const int c = node * 32 + lane;
+    stat_add<S>(s, lane, kStatNodes, 1);
     bool pass = false;
-    if (c < m.lvl_cnt[cl]) {
-      const int j = m.lvl_off[cl] + c;
-      const float4 lo = __ldg(m.boxes + 2 * j);
-      const float4 hi = __ldg(m.boxes + 2 * j + 1);
-      pass = box_dist2(qx, qy, qz, lo, hi) <= tau;
+    if (c < L.cnt[cl]) {
+      const int jb = L.off[cl] + c;
+      const float4 lo = __ldg(m.boxes + 2 * jb);
+      const float4 hi = __ldg(m.boxes + 2 * jb + 1);
+      pass = box_dist2(q.x, q.y, q.z, lo, hi) <= q.tau;
     }
-    unsigned bal = __ballot_sync(kFull, pass);
+    const unsigned bal = __ballot_sync(kFull, pass);
     if (cl == 0) {
-      while (bal) {
-        const int b = __ffs(bal) - 1;
-        bal &= bal - 1;
-        scan_leaf(m, node * 32 + b, qx, qy, qz, tau, cnt, s, lane, k);
-      }
+      if (pass) s.list[__popc(bal & lanemask_lt())] = (uint32_t)c;
+      __syncwarp();
+      if (bal) scan_groups<C, S>(m, q, s, lane, __popc(bal));
     } else {
       if (pass)
         s.stack[sp + __popc(bal & lanemask_lt())] = ((uint32_t)cl << 28) | c;
@@ -455,7 +650,6 @@ __device__ int collect(const MapDev& m, float qx, float qy, float qz,
       __syncwarp();
     }
   }
-  return cnt;
 }
 
 __device__ __forceinline__ unsigned long long warp_min_u64(
@@ -468,49 +662,75 @@ __device__ __forceinline__ unsigned long long warp_min_u64(
   return v;
 }
 
-// Upper bound of the k-th distance from scratch: walk down to the nearest
-// box greedily, then take the k-th distance among the photons of the
-// leaves around it (real photons, so the bound is valid).
-template <int C>
-__device__ float cold_tau(const MapDev& m, float qx, float qy, float qz,
-                          WarpBuf<C>& s, int lane, int k) {
+// Upper bound of the k-th distance from scratch: walk down to a group
+// greedily (nearest box at each level), then take the k-th distance among
+// the photons of the Morton-adjacent groups around it (real photons, so
+// the bound holds).
+template <int C, bool S>
+__device__ __forceinline__ float cold_tau(const float4* pos4, const float4* boxes,
+                                       int n, int nlevels, const Levels* Lp,
+                                       float qx, float qy, float qz, int k,
+                                       WarpBuf<C>* sp, int lane) {
+  const Levels& L = *Lp;
+  WarpBuf<C>& s = *sp;
   int node = 0;
-  for (int lvl = m.nlevels - 1; lvl >= 1; --lvl) {
-    const int cl = lvl - 1;
+  for (int cl = nlevels - 2; cl >= 0; --cl) {
     const int c = node * 32 + lane;
     unsigned long long key = ~0ull;
-    if (c < m.lvl_cnt[cl]) {
-      const int j = m.lvl_off[cl] + c;
-      const float d = box_dist2(qx, qy, qz, __ldg(m.boxes + 2 * j),
-                                __ldg(m.boxes + 2 * j + 1));
+    if (c < L.cnt[cl]) {
+      const int jb = L.off[cl] + c;
+      const float d = box_dist2(qx, qy, qz, __ldg(boxes + 2 * jb),
+                                __ldg(boxes + 2 * jb + 1));
       key = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)c;
     }
     key = warp_min_u64(key);
     node = (int)(key & 0xffffffffu);
   }
-  const int nleaves = m.lvl_cnt[0];
-  const int want = min(nleaves, (k + 31) / 32 + 2);
-  const int first = max(0, min(node - want / 2, nleaves - want));
-  float tau = __int_as_float(0x7f800000);  // +inf
-  int cnt = 0;
-  for (int l = first; l < first + want; ++l)
-    scan_leaf(m, l, qx, qy, qz, tau, cnt, s, lane, k);
+  MapDev m;
+  m.pos4 = pos4;
+  m.n = n;
+  Query q;
+  q.x = qx; q.y = qy; q.z = qz;
+  q.k = k;
+  q.tau = __int_as_float(0x7f800000);  // +inf
+  q.cnt = 0;
+  // the photons of the 32 groups sharing the nearest group's parent (a
+  // compact patch of 256 Morton-adjacent photons), or more groups around
+  // it when k needs them
+  const int ngroups = L.cnt[0];
+  const int want = min(ngroups, max(32, (k + kGroup - 1) / kGroup + 8));
+  const int first =
+      max(0, min(want == 32 ? (node & ~31) : node - want / 2, ngroups - want));
+  scan_range<C, S>(m, q, s, lane, first * kGroup, min(n, (first + want) * kGroup));
   __syncwarp();
-  if (cnt < k) return __int_as_float(0x7f800000);
+  if (q.cnt < k) return __int_as_float(0x7f800000);
+  uint32_t mx = 0;
+  for (int i = lane; i < q.cnt; i += 32) mx = max(mx, s.key[i]);
+  mx = __reduce_max_sync(kFull, mx);  // every entry lies in [0, mx]
   uint32_t kth_key, kth_oid;
-  select_kth(m, s, cnt, k, lane, kth_key, kth_oid);
+  select_kth<C, S>(pos4, s, q.cnt, k, __uint_as_float(mx), lane, kth_key, kth_oid);
   return __uint_as_float(kth_key);
 }
 
-template <int C, int MODE>
-__global__ void __launch_bounds__(256)
+template <int C, int MODE, bool S>
+__global__ void __launch_bounds__(256, 4)
     knn_kernel(MapDev m, const void* __restrict__ queries, int64_t nq, int k,
                float n_emitted, KnnOut out,
                unsigned long long* __restrict__ counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ Levels L;
   WarpBuf<C>& s = reinterpret_cast<WarpBuf<C>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
   const float kInf = __int_as_float(0x7f800000);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < kMaxLevels; ++i) {  // constant indices: m stays in
+      L.off[i] = m.lvl_off[i];              // the parameter bank
+      L.cnt[i] = m.lvl_cnt[i];
+    }
+  }
+  if (lane < 8) s.stat[lane] = 0;
+  __syncthreads();
 
   while (true) {
     unsigned long long c0 = 0;
@@ -523,41 +743,45 @@ __global__ void __launch_bounds__(256)
     bool have_prev = false;
     float pqx = 0.f, pqy = 0.f, pqz = 0.f, pkth = 0.f;
     for (int64_t qi = qb; qi < qe; ++qi) {
-      float qx, qy, qz;
-      // radiance records: r0 = {pos, rho.r}, r1 = {wo, rho.g},
-      // r2 = {ns, rho.b}
-      float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f), r1 = r0, r2 = r0;
+      Query q;
+      q.k = k;
+      q.cnt = 0;
+      q.tau = kInf;
       if (MODE == kModeRadiance) {
-        const float4* q4 = reinterpret_cast<const float4*>(queries) + 3 * qi;
-        r0 = __ldg(q4);
-        r1 = __ldg(q4 + 1);
-        r2 = __ldg(q4 + 2);
-        qx = r0.x; qy = r0.y; qz = r0.z;
+        // radiance record r0 = {pos, rho.r}; wo, ns and the other albedo
+        // channels are read after the search
+        const float4 r0 = __ldg(reinterpret_cast<const float4*>(queries) + 3 * qi);
+        q.x = r0.x; q.y = r0.y; q.z = r0.z;
       } else {
         const float* q3 = reinterpret_cast<const float*>(queries) + 3 * qi;
-        qx = __ldg(q3);
-        qy = __ldg(q3 + 1);
-        qz = __ldg(q3 + 2);
+        q.x = __ldg(q3);
+        q.y = __ldg(q3 + 1);
+        q.z = __ldg(q3 + 2);
       }
 
-      int cnt = 0;
-      float tau = kInf;
-      const bool bad = m.n == 0 || isnan(qx) || isnan(qy) || isnan(qz);
+      const bool bad = m.n == 0 || isnan(q.x) || isnan(q.y) || isnan(q.z);
       if (!bad) {
         bool warm = false;
         if (have_prev) {
-          const float d2 = dist2_ref(qx, qy, qz, pqx, pqy, pqz);
+          const float d2 = dist2_ref(q.x, q.y, q.z, pqx, pqy, pqz);
           if (d2 <= pkth) {
             const float r = sqrtf(pkth) + sqrtf(d2);
             const float rr = r * 1.00001f;
-            tau = fmaxf(rr * rr * 1.00001f, 1e-37f);
+            q.tau = fmaxf(rr * rr * 1.00001f, 1e-37f);
             warm = true;
           }
         }
-        if (!warm) tau = cold_tau(m, qx, qy, qz, s, lane, k);
-        cnt = collect(m, qx, qy, qz, tau, s, lane, k);
+        if (!warm) {
+          stat_add<S>(s, lane, kStatCold, 1);
+          q.tau = cold_tau<C, S>(m.pos4, m.boxes, m.n, m.nlevels, &L, q.x, q.y,
+                              q.z, k, &s, lane);
+        }
+        collect<C, S>(m, L, q, s, lane);
       }
       __syncwarp();
+      stat_add<S>(s, lane, kStatQueries, 1);
+      stat_add<S>(s, lane, kStatCand, (uint32_t)q.cnt);
+      const int cnt = q.cnt;
 
       // final selection
       const bool all = cnt <= k;
@@ -567,12 +791,17 @@ __global__ void __launch_bounds__(256)
         for (int i = lane; i < cnt; i += 32) mx = max(mx, s.key[i]);
         kth_key = __reduce_max_sync(kFull, mx);
       } else {
-        select_kth(m, s, cnt, k, lane, kth_key, kth_oid);
+        select_kth<C, S>(m.pos4, s, cnt, k, q.tau, lane, kth_key, kth_oid);
       }
       const int kept = all ? cnt : k;
       const float maxd2 = kept > 0 ? __uint_as_float(kth_key) : 0.f;
 
       if (MODE == kModeRadiance) {
+        // r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b}
+        const float4* q4 = reinterpret_cast<const float4*>(queries) + 3 * qi;
+        const float4 r0 = __ldg(q4);
+        const float4 r1 = __ldg(q4 + 1);
+        const float4 r2 = __ldg(q4 + 2);
         const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
         const float fr = __fdiv_rn(r0.w, kPI);
         const float fg = __fdiv_rn(r1.w, kPI);
@@ -581,7 +810,7 @@ __global__ void __launch_bounds__(256)
         for (int i = lane; i < cnt; i += 32) {
           const uint32_t key = s.key[i];
           const uint32_t id = s.id[i];
-          if (all || keep_entry(m, key, id, kth_key, kth_oid)) {
+          if (all || keep_entry(m.pos4, key, id, kth_key, kth_oid)) {
             const float4 t = __ldg(m.thr4 + id);
             const float2 w = __ldg(m.wi2 + id);
             const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
@@ -612,8 +841,9 @@ __global__ void __launch_bounds__(256)
         }
       } else {
         int n2 = cnt;
-        if (!all) n2 = compact_kept(m, s, cnt, kth_key, kth_oid, lane);
-        for (int i = lane; i < n2; i += 32) s.id[i] = orig_index(m, s.id[i]);
+        if (!all) n2 = compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
+        for (int i = lane; i < n2; i += 32)
+          s.id[i] = orig_index(m.pos4, s.id[i]);
         __syncwarp();
         int32_t* orow = out.idx + qi * (int64_t)k;
         for (int i = lane; i < n2; i += 32) {
@@ -635,11 +865,19 @@ __global__ void __launch_bounds__(256)
 
       if (!bad && kept >= k) {
         have_prev = true;
-        pqx = qx; pqy = qy; pqz = qz;
+        pqx = q.x; pqy = q.y; pqz = q.z;
         pkth = maxd2;
       } else {
         have_prev = false;
       }
+    }
+    if (S) {
+      __syncwarp();
+      if (lane < 6) {
+        atomicAdd(out.stats + lane, (unsigned long long)s.stat[lane]);
+        s.stat[lane] = 0;
+      }
+      __syncwarp();
     }
   }
 }
@@ -651,7 +889,7 @@ static cudaError_t launch_one(const MapDev& m, const void* queries,
                               cudaStream_t st) {
   constexpr int kThreads = (C <= 512) ? 256 : 128;
   const size_t smem = (kThreads / 32) * sizeof(WarpBuf<C>);
-  auto kern = knn_kernel<C, MODE>;
+  auto kern = out.stats ? knn_kernel<C, MODE, true> : knn_kernel<C, MODE, false>;
   cudaError_t e = cudaFuncSetAttribute(
       kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -678,7 +916,7 @@ cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                        unsigned long long* counter, int num_sms,
                        cudaStream_t st) {
   if (nq <= 0) return cudaSuccess;
-  if (k <= 256) {
+  if (k <= 224) {
     return mode == kModeRadiance
                ? launch_one<512, kModeRadiance>(m, queries, nq, k, n_emitted,
                                                 out, counter, num_sms, st)

@@ -11,9 +11,9 @@
 //   thr4   float4[n]   same order: {throughput.rgb, wi.x}
 //   wi2    float2[n]   same order: {wi.y, wi.z}
 //   boxes  float4[2m]  32-ary box tree over the sorted array: level 0 has
-//                      one box per 32-photon leaf, level l+1 one box per 32
-//                      level-l boxes; node j of all levels is {lo, hi} at
-//                      boxes[2j], boxes[2j+1].
+//                      one box per group of 8 consecutive photons, level
+//                      l+1 one box per 32 level-l boxes; node j of all
+//                      levels is {lo, hi} at boxes[2j], boxes[2j+1].
 #pragma once
 
 #include "pm_common.cuh"
@@ -21,6 +21,7 @@
 namespace pm {
 
 constexpr int kMaxLevels = 8;
+constexpr int kGroup = 8;  // photons per bottom-level box
 
 struct MapDev {
   const float4* __restrict__ pos4;
@@ -52,6 +53,7 @@ struct KnnOut {
   int32_t* idx;        // knn mode: k per query
   int32_t* count;      // knn mode
   float* maxd2;        // knn mode
+  unsigned long long* stats;  // 6 counters (pm_knn_stats) or null
 };
 
 // Launches the warp-per-query k-nearest-neighbour kernel.
