@@ -139,6 +139,57 @@ int pm_photonmap_radiance_device(pm_ctx* ctx, int map, const void* d_queries,
                                  int64_t nq, int k, int64_t n_emitted,
                                  void* d_out_rgb, void* stream);
 
+/* --------------------------------------------------------------- scene */
+/* Per-face material, as Scene::loadModel derives it from the OBJ/MTL
+ * (scene.h:15-51): illum 5 -> Mirror, illum 7 -> Glass(Ni), otherwise
+ * Lambert(Kd); Ke > 0 makes the face an area light (AreaLight, light.h). */
+enum pm_material_type { PM_LAMBERT = 0, PM_MIRROR = 1, PM_GLASS = 2 };
+typedef struct pm_material {
+  int32_t type;   /* pm_material_type                                      */
+  float rho[3];   /* albedo; Mirror and Glass use (1, 1, 1) (scene.h:26-33) */
+  float ior;      /* Glass index of refraction                             */
+  float le[3];    /* emitted radiance; light when any component > 0        */
+} pm_material;
+
+/* Replaces Scene::build (scene.h:275-304): uploads the faces and builds the
+ * device LBVH. vertices and normals hold 9 floats per face (the reference's
+ * per-face unshared vertices, scene.h:199-212; a face without normals
+ * carries its geometric normal three times, scene.h:182-189). */
+int pm_scene_upload(pm_ctx* ctx, const float* vertices, const float* normals,
+                    const pm_material* materials, int64_t n_faces);
+
+/* Closest hit of a ray (Scene::intersect, scene.h:307-348). */
+typedef struct pm_hit {
+  float t;        /* hit distance; hit point = origin + t * direction      */
+  float u, v;     /* barycentrics of vertices 1 and 2 (Embree's u, v)      */
+  int32_t prim;   /* face index, -1 when nothing was hit                   */
+} pm_hit;
+
+/* Batched Scene::intersect. rays: 8 floats each {origin.xyz, tmin,
+ * direction.xyz, tmax}; a hit needs tmin <= t <= tmax. Among hits at the
+ * same distance the smallest face index is returned. */
+int pm_scene_intersect(pm_ctx* ctx, const float* rays, int64_t n,
+                       pm_hit* out);
+
+/* ------------------------------------------------------ photon tracing */
+typedef struct pm_trace_stats {
+  int64_t emitted;              /* photons emitted                       */
+  int64_t stored;               /* photons stored in the map             */
+  uint32_t nan_throughput;      /* paths stopped on a NaN throughput     */
+  uint32_t negative_throughput; /* paths stopped on a negative one       */
+} pm_trace_stats;
+
+/* Replaces the photon-tracing half of PhotonMapping::build
+ * (integrator.h:393-563): emits n_emit photons from the scene's area lights
+ * and traces them for at most max_depth (<= 255) bounces with the storage
+ * rule of `map` (PM_MAP_GLOBAL: every diffuse hit, integrator.h:406-469;
+ * PM_MAP_CAUSTICS: the first diffuse hit after a specular one,
+ * integrator.h:483-558), then builds that photon map. Photon i draws from
+ * its own PCG32 stream (state derived from seed and i), so the stored set
+ * and its order (by photon, then bounce) are reproducible. */
+int pm_photons_trace(pm_ctx* ctx, int map, uint64_t seed, int64_t n_emit,
+                     int max_depth, pm_trace_stats* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -49,6 +49,11 @@ def oracle_lib() -> C.CDLL:
             "orc_knn": (None, [_vp, _i64, _vp, _i64, C.c_int, _vp, _vp, _vp]),
             "orc_radiance_fp64": (None, [_vp, _vp, _vp, _vp, C.c_int, _vp, _i64, _i64, _vp]),
             "orc_radiance_fp32": (None, [_vp, _vp, _vp, _vp, C.c_int, _vp, _i64, _i64, _vp]),
+            "orc_scene_new": (_vp, [_vp, _vp, _vp, _i64]),
+            "orc_scene_free": (None, [_vp]),
+            "orc_intersect": (None, [_vp, _vp, _i64, _vp]),
+            "orc_trace": (_i64, [_vp, C.c_int, C.c_uint64, _i64, _i64, C.c_int, _vp, _i64, _vp]),
+            "orc_sincos": (None, [_vp, _i64, _vp, _vp]),
         })
     return _oracle
 
@@ -148,3 +153,52 @@ class RefPhotonMap:
 
 def ref_threads() -> int:
     return int(ref_pm_lib().ref_max_threads())
+
+
+class OracleScene:
+    """CPU restatement of the scene: brute-force closest hit and the
+    reference's photon tracing loops (oracle/pm_oracle_trace.cpp)."""
+
+    def __init__(self, mesh):
+        self.lib = oracle_lib()
+        self.v = _c(mesh.vertices, np.float32)
+        self.n = _c(mesh.normals, np.float32)
+        self.m = np.ascontiguousarray(mesh.materials)
+        self.h = self.lib.orc_scene_new(self.v.ctypes.data, self.n.ctypes.data,
+                                        self.m.ctypes.data, self.v.shape[0])
+
+    def intersect(self, rays8):
+        r = _c(rays8, np.float32).reshape(-1, 8)
+        out = np.empty((r.shape[0], 4), np.float32)
+        self.lib.orc_intersect(self.h, r.ctypes.data, r.shape[0], out.ctypes.data)
+        return out
+
+    def trace(self, map_id: int, seed: int, first: int, count: int, max_depth: int,
+              cap: int | None = None):
+        cap = cap if cap is not None else max(16, count * 8)
+        out = np.empty((cap, 9), np.float32)
+        st = np.zeros(2, np.uint32)
+        n = self.lib.orc_trace(self.h, map_id, seed, first, count, max_depth, out.ctypes.data,
+                               cap, st.ctypes.data)
+        if n > cap:
+            return self.trace(map_id, seed, first, count, max_depth, cap=n)
+        return out[:n], st
+
+    def close(self):
+        if self.h:
+            self.lib.orc_scene_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def sincos(x):
+    x = _c(x, np.float32).ravel()
+    s = np.empty_like(x)
+    c = np.empty_like(x)
+    oracle_lib().orc_sincos(x.ctypes.data, x.shape[0], s.ctypes.data, c.ctypes.data)
+    return s, c

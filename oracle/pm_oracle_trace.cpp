@@ -1,0 +1,412 @@
+// ORACLE — test infrastructure only. CPU restatement of the reference's
+// scene intersection and photon tracing, used by tests/ as the checker of
+// the device LBVH and photon tracer. Built with -ffp-contract=off.
+//
+// Follows yumcyaWiz/photon_mapping:
+//   scene.h:307-355     intersect (closest hit) and sampleLight
+//   triangle.h:25-114   geometric normal, area, shading normal, samplePoint
+//   light.h:27-44       AreaLight Le and sampleDirection
+//   material.h          Lambert, Mirror, Glass
+//   primitive.h:32-82   world/local frames
+//   integrator.h:25-46  cosTerm
+//   integrator.h:265-288, 393-563  sampleRayFromLight and the two tracing loops
+//   sampler.h:11-91     PCG32 (state = seed, inc = 1) and sampleCosineHemisphere
+//
+// Choices shared with the device code (the definition of the path, not the
+// reference's): the intersector is Moller-Trumbore with tmin <= t <= tmax
+// and ties in t broken by the smaller face index (Embree itself is absent);
+// cos/sin(theta) of the cosine hemisphere use the closed forms sqrt(1-u),
+// sqrt(u) of cos/sin(acos(1-2u)/2); sin/cos(phi) come from a double-precision
+// Taylor evaluation; photon i uses the stream state
+// splitmix64(seed ^ splitmix64(i)); getNext2D returns (second, first) draw,
+// the argument order the reference's GCC build evaluates.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace orc {
+
+struct V {
+  float x, y, z;
+};
+static inline V mk(float x, float y, float z) { return V{x, y, z}; }
+static inline V add(V a, V b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline V sub(V a, V b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline V neg(V a) { return mk(-a.x, -a.y, -a.z); }
+static inline V mul(V a, V b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline V muls(V a, float k) { return mk(a.x * k, a.y * k, a.z * k); }
+static inline V divs(V a, float k) { return mk(a.x / k, a.y / k, a.z / k); }
+static inline float dot(V a, V b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline V cross(V a, V b) {
+  return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+static inline float length(V a) { return std::sqrt(dot(a, a)); }
+static inline V normalize(V a) { return divs(a, length(a)); }
+static inline void basis(V n, V& t, V& b) {
+  if (std::fabs(n.y) < 0.9f)
+    t = normalize(cross(n, mk(0, 1, 0)));
+  else
+    t = normalize(cross(n, mk(0, 0, -1)));
+  b = normalize(cross(t, n));
+}
+static inline V to_local(V v, V lx, V ly, V lz) {
+  return mk(dot(v, lx), dot(v, ly), dot(v, lz));
+}
+static inline V to_world(V v, V lx, V ly, V lz) {
+  return mk(v.x * lx.x + v.y * ly.x + v.z * lz.x, v.x * lx.y + v.y * ly.y + v.z * lz.y,
+            v.x * lx.z + v.y * ly.z + v.z * lz.z);
+}
+
+constexpr float PI = 3.14159265359f;
+constexpr float PI_INV = 1.0f / PI;
+constexpr float PI_MUL_2 = 2.0f * PI;
+constexpr float RAY_EPS = 1e-5f;
+
+struct Rng {
+  uint64_t state;
+  uint32_t u32() {
+    const uint64_t old = state;
+    state = old * 6364136223846793005ULL + 1ULL;
+    const uint32_t xs = (uint32_t)(((old >> 18u) ^ old) >> 27u);
+    const uint32_t rot = (uint32_t)(old >> 59u);
+    return (xs >> rot) | (xs << ((0u - rot) & 31u));
+  }
+  float next() { return (float)u32() * (1.0f / 4294967295.0f); }
+  void next2(float& u0, float& u1) {
+    u1 = next();
+    u0 = next();
+  }
+};
+
+static inline uint64_t splitmix64(uint64_t x) {
+  x += 0x9E3779B97F4A7C15ULL;
+  x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  x = (x ^ (x >> 27)) * 0x94D049BB133111EBULL;
+  return x ^ (x >> 31);
+}
+
+// sin/cos of a float angle: reduction by pi/2 and Taylor series in double.
+static inline void sincos_d(float xf, float& s, float& c) {
+  const double x = (double)xf;
+  const double q = std::rint(x * 0.63661977236758134308);
+  const double r = x - q * 1.5707963267948966192;
+  const double r2 = r * r;
+  static const double sin_inv_fact[9] = {
+      1.0 / 355687428096000.0, 1.0 / 1307674368000.0, 1.0 / 6227020800.0,
+      1.0 / 39916800.0,        1.0 / 362880.0,        1.0 / 5040.0,
+      1.0 / 120.0,             1.0 / 6.0,             1.0};
+  static const double cos_inv_fact[9] = {
+      1.0 / 6402373705728000.0, 1.0 / 20922789888000.0, 1.0 / 87178291200.0,
+      1.0 / 479001600.0,        1.0 / 3628800.0,        1.0 / 40320.0,
+      1.0 / 720.0,              1.0 / 24.0,             1.0 / 2.0};
+  double ps = sin_inv_fact[0];
+  for (int i = 1; i < 9; ++i) ps = ps * -r2 + sin_inv_fact[i];
+  const double sr = r * ps;
+  double pc = cos_inv_fact[0];
+  for (int i = 1; i < 9; ++i) pc = pc * -r2 + cos_inv_fact[i];
+  const double cr = 1.0 - r2 * pc;
+  const int quad = ((int)q) & 3;
+  double sd = sr, cd = cr;
+  if (quad == 1) { sd = cr; cd = -sr; }
+  else if (quad == 2) { sd = -sr; cd = -cr; }
+  else if (quad == 3) { sd = -cr; cd = sr; }
+  s = (float)sd;
+  c = (float)cd;
+}
+
+static inline V cos_hemisphere(float u0, float u1, float& pdf) {
+  const float ct = std::sqrt(1.0f - u0);
+  const float st = std::sqrt(u0);
+  const float phi = PI_MUL_2 * u1;
+  float sp, cp;
+  sincos_d(phi, sp, cp);
+  pdf = PI_INV * ct;
+  return mk(cp * st, ct, sp * st);
+}
+
+struct Mat {
+  int32_t type;
+  float rho[3];
+  float ior;
+  float le[3];
+};
+
+struct Scene {
+  int n = 0;
+  std::vector<V> p, nrm;  // 3 per face
+  std::vector<V> gn;      // geometric normal
+  std::vector<float> area;
+  std::vector<V> e1, e2;
+  std::vector<Mat> mat;
+  std::vector<int> lights;
+};
+
+struct Hit {
+  float t, u, v;
+  int prim;
+};
+
+static bool intersect(const Scene& s, V o, V d, float tmin, float tmax, Hit& h) {
+  h.prim = -1;
+  h.t = tmax;
+  h.u = h.v = 0.f;
+  for (int f = 0; f < s.n; ++f) {
+    const V p0 = s.p[3 * f];
+    const V pvec = cross(d, s.e2[f]);
+    const float det = dot(s.e1[f], pvec);
+    if (!(det != 0.f)) continue;
+    const float inv = 1.0f / det;
+    const V tvec = sub(o, p0);
+    const float u = dot(tvec, pvec) * inv;
+    if (!(u >= 0.f && u <= 1.f)) continue;
+    const V qvec = cross(tvec, s.e1[f]);
+    const float v = dot(d, qvec) * inv;
+    if (!(v >= 0.f && u + v <= 1.f)) continue;
+    const float t = dot(s.e2[f], qvec) * inv;
+    if (!(t == t)) continue;
+    if (t >= tmin && t <= h.t && (t < h.t || h.prim < 0)) {
+      h.t = t;
+      h.u = u;
+      h.v = v;
+      h.prim = f;
+    }
+  }
+  return h.prim >= 0;
+}
+
+struct Surf {
+  V pos, ng, ns, dpdu, dpdv;
+};
+
+static inline V shading_normal(const Scene& s, int f, float b0, float b1) {
+  return add(add(muls(s.nrm[3 * f], 1.0f - b0 - b1), muls(s.nrm[3 * f + 1], b0)),
+             muls(s.nrm[3 * f + 2], b1));
+}
+
+static Surf surface(const Scene& s, V o, V d, const Hit& h) {
+  Surf r;
+  r.pos = add(o, muls(d, h.t));
+  r.ng = s.gn[h.prim];
+  r.ns = shading_normal(s, h.prim, h.u, h.v);
+  basis(r.ns, r.dpdu, r.dpdv);
+  return r;
+}
+
+static inline V rho(const Mat& m) { return mk(m.rho[0], m.rho[1], m.rho[2]); }
+
+static inline V lambert_eval(const Mat& m, V wo, V wi) {
+  if (wo.y < 0 || wi.y < 0) return mk(0, 0, 0);
+  return divs(rho(m), PI);
+}
+
+static inline V reflect(V v, V n) { return add(neg(v), muls(n, 2.0f * dot(v, n))); }
+
+static inline bool refract(V v, V n, float iorI, float iorT, V& t) {
+  const V th = muls(sub(v, muls(n, dot(v, n))), -iorI / iorT);
+  if (dot(th, th) > 1.0f) return false;
+  const V tp = muls(n, -std::sqrt(std::max(1.0f - dot(th, th), 0.0f)));
+  t = add(th, tp);
+  return true;
+}
+
+static inline float fresnel(float c, float iorI, float iorT) {
+  const float f0 = (iorI - iorT) * (iorI - iorT) / ((iorI + iorT) * (iorI + iorT));
+  const float x = std::max(1.0f - std::fabs(c), 0.0f);
+  return f0 + (1.0f - f0) * (x * x * x * x * x);
+}
+
+// FROM_LIGHT = 0, FROM_CAMERA = 1
+static V sample_bxdf(const Mat& m, V wo, int tdir, Rng& rng, V& wi, float& pdf) {
+  if (m.type == 0) {
+    float u0, u1;
+    rng.next2(u0, u1);
+    wi = cos_hemisphere(u0, u1, pdf);
+    return lambert_eval(m, wo, wi);
+  }
+  if (m.type == 1) {
+    wi = reflect(wo, mk(0, 1, 0));
+    pdf = 1.0f;
+    return divs(rho(m), std::fabs(wi.y));
+  }
+  float iorO, iorI;
+  V n;
+  if (wo.y > 0) {
+    iorO = 1.0f; iorI = m.ior; n = mk(0, 1, 0);
+  } else {
+    iorO = m.ior; iorI = 1.0f; n = mk(0, -1, 0);
+  }
+  const float fr = fresnel(dot(wo, n), iorO, iorI);
+  if (rng.next() < fr) {
+    wi = reflect(wo, n);
+    pdf = 1.0f;
+    return divs(rho(m), std::fabs(wi.y));
+  }
+  V tr;
+  if (refract(wo, n, iorO, iorI, tr)) {
+    wi = tr;
+    pdf = 1.0f;
+    float sc = 1.0f;
+    if (tdir == 1) sc = (iorO * iorO) / (iorI * iorI);
+    return divs(muls(rho(m), sc), std::fabs(wi.y));
+  }
+  wi = reflect(wo, n);
+  pdf = 1.0f;
+  return divs(rho(m), std::fabs(wi.y));
+}
+
+static inline float cos_term(V wo, V wi, V ns, V ng, int tdir) {
+  const float wi_ns = dot(wi, ns), wi_ng = dot(wi, ng);
+  const float wo_ns = dot(wo, ns), wo_ng = dot(wo, ng);
+  if (wi_ng * wi_ns <= 0 || wo_ng * wo_ns <= 0) return 0;
+  if (tdir == 1) return std::fabs(wi_ns);
+  return std::fabs(wo_ns) * std::fabs(wi_ng) / std::fabs(wo_ng);
+}
+
+static Surf sample_point(const Scene& s, int f, Rng& rng, float& pdf) {
+  float u0, u1;
+  rng.next2(u0, u1);
+  const float su0 = std::sqrt(u0);
+  const float b0 = 1.0f - su0, b1 = u1 * su0;
+  Surf r;
+  r.pos = add(add(muls(s.p[3 * f], 1.0f - b0 - b1), muls(s.p[3 * f + 1], b0)),
+              muls(s.p[3 * f + 2], b1));
+  r.ns = shading_normal(s, f, b0, b1);
+  basis(r.ns, r.dpdu, r.dpdv);
+  r.ng = s.gn[f];
+  pdf = 1.0f / s.area[f];
+  return r;
+}
+
+static int sample_light(const Scene& s, Rng& rng, float& pdf) {
+  unsigned idx = (unsigned)((float)s.lights.size() * rng.next());
+  if (idx == s.lights.size()) idx--;
+  pdf = 1.0f / (float)s.lights.size();
+  return s.lights[idx];
+}
+
+}  // namespace orc
+
+using namespace orc;
+
+extern "C" {
+
+void* orc_scene_new(const float* verts, const float* nrms, const void* mats,
+                    int64_t n) {
+  Scene* s = new Scene();
+  s->n = (int)n;
+  const Mat* m = (const Mat*)mats;
+  for (int64_t f = 0; f < n; ++f) {
+    for (int k = 0; k < 3; ++k) {
+      s->p.push_back(mk(verts[9 * f + 3 * k], verts[9 * f + 3 * k + 1], verts[9 * f + 3 * k + 2]));
+      s->nrm.push_back(mk(nrms[9 * f + 3 * k], nrms[9 * f + 3 * k + 1], nrms[9 * f + 3 * k + 2]));
+    }
+    const V p1 = s->p[3 * f], p2 = s->p[3 * f + 1], p3 = s->p[3 * f + 2];
+    const V c = cross(sub(p2, p1), sub(p3, p1));  // triangle.h:30-33
+    s->gn.push_back(normalize(c));
+    s->area.push_back(0.5f * length(c));
+    s->e1.push_back(sub(p2, p1));
+    s->e2.push_back(sub(p3, p1));
+    s->mat.push_back(m[f]);
+    if (m[f].le[0] > 0 || m[f].le[1] > 0 || m[f].le[2] > 0) s->lights.push_back((int)f);
+  }
+  return s;
+}
+
+void orc_scene_free(void* h) { delete (Scene*)h; }
+
+// rays: 8 floats {origin, tmin, direction, tmax}; out: 4 words {t, u, v, prim}
+void orc_intersect(void* h, const float* rays, int64_t n, float* out) {
+  const Scene& s = *(const Scene*)h;
+#pragma omp parallel for schedule(dynamic, 256)
+  for (int64_t i = 0; i < n; ++i) {
+    const float* r = rays + 8 * i;
+    Hit hit;
+    const bool ok = intersect(s, mk(r[0], r[1], r[2]), mk(r[4], r[5], r[6]), r[3], r[7], hit);
+    float* o = out + 4 * i;
+    o[0] = ok ? hit.t : 0.f;
+    o[1] = ok ? hit.u : 0.f;
+    o[2] = ok ? hit.v : 0.f;
+    int32_t prim = ok ? hit.prim : -1;
+    std::memcpy(o + 3, &prim, 4);
+  }
+}
+
+// Photon tracing of integrator.h:393-563 for photons [first, first+count)
+// of a trace seeded with `seed`; map 0 = global rule, 1 = caustics rule.
+// Writes up to cap photons (9 floats) in (photon, bounce) order; returns the
+// number stored (which may exceed cap). status[0..1]: NaN / negative stops.
+int64_t orc_trace(void* h, int map, uint64_t seed, int64_t first, int64_t count,
+                  int max_depth, float* out, int64_t cap, uint32_t* status) {
+  const Scene& s = *(const Scene*)h;
+  int64_t stored = 0;
+  status[0] = status[1] = 0;
+  auto store = [&](V thr, V pos, V wi) {
+    if (stored < cap) {
+      float* o = out + 9 * stored;
+      o[0] = thr.x; o[1] = thr.y; o[2] = thr.z;
+      o[3] = pos.x; o[4] = pos.y; o[5] = pos.z;
+      o[6] = wi.x; o[7] = wi.y; o[8] = wi.z;
+    }
+    ++stored;
+  };
+  for (int64_t i = first; i < first + count; ++i) {
+    Rng rng{splitmix64(seed ^ splitmix64((uint64_t)i))};
+    float pc, pp, pd;
+    const int lf = sample_light(s, rng, pc);
+    const Surf ls = sample_point(s, lf, rng, pp);
+    float u0, u1;
+    rng.next2(u0, u1);
+    V dir = to_world(cos_hemisphere(u0, u1, pd), ls.dpdu, ls.ns, ls.dpdv);
+    const Mat& lm = s.mat[lf];
+    V thr = muls(divs(mk(lm.le[0], lm.le[1], lm.le[2]), pc * pp * pd), std::fabs(dot(dir, ls.ns)));
+    V org = ls.pos;
+    bool prev_specular = false;
+    for (int k = 0; k < max_depth; ++k) {
+      if (std::isnan(thr.x) || std::isnan(thr.y) || std::isnan(thr.z)) {
+        status[0]++;
+        break;
+      }
+      if (thr.x < 0 || thr.y < 0 || thr.z < 0) {
+        status[1]++;
+        break;
+      }
+      Hit hit;
+      if (!intersect(s, org, dir, RAY_EPS, 3.40282347e+38f, hit)) break;
+      const Surf sf = surface(s, org, dir, hit);
+      const Mat& m = s.mat[hit.prim];
+      const bool diffuse = m.type == 0;
+      if (map == 0) {
+        if (diffuse) store(thr, sf.pos, neg(dir));
+      } else {
+        if (!prev_specular && diffuse) break;
+        if (prev_specular && diffuse) {
+          store(thr, sf.pos, neg(dir));
+          break;
+        }
+        prev_specular = !diffuse;
+      }
+      if (k > 0) {
+        const float q = std::min(std::max(thr.x, std::max(thr.y, thr.z)), 1.0f);
+        if (rng.next() >= q) break;
+        thr = divs(thr, q);
+      }
+      const V wo = neg(dir);
+      V wil;
+      float pdf;
+      const V f = sample_bxdf(m, to_local(wo, sf.dpdu, sf.ns, sf.dpdv), 0, rng, wil, pdf);
+      const V wi = to_world(wil, sf.dpdu, sf.ns, sf.dpdv);
+      thr = mul(thr, divs(muls(f, cos_term(wo, wi, sf.ns, sf.ng, 0)), pdf));
+      org = sf.pos;
+      dir = wi;
+    }
+  }
+  return stored;
+}
+
+// sin and cos of n float angles with the double-precision evaluation above.
+void orc_sincos(const float* x, int64_t n, float* s, float* c) {
+  for (int64_t i = 0; i < n; ++i) sincos_d(x[i], s[i], c[i]);
+}
+
+}  // extern "C"

@@ -57,6 +57,9 @@ _SIGNATURES = {
     "pm_photonmap_knn": (C.c_int, [_vp, C.c_int, _vp, _i64, C.c_int, _vp, _vp, _vp]),
     "pm_photonmap_radiance": (C.c_int, [_vp, C.c_int, _vp, _i64, C.c_int, _i64, _vp]),
     "pm_photonmap_radiance_device": (C.c_int, [_vp, C.c_int, _vp, _i64, C.c_int, _i64, _vp, _vp]),
+    "pm_scene_upload": (C.c_int, [_vp, _vp, _vp, _vp, _i64]),
+    "pm_scene_intersect": (C.c_int, [_vp, _vp, _i64, _vp]),
+    "pm_photons_trace": (C.c_int, [_vp, C.c_int, C.c_uint64, _i64, C.c_int, _vp]),
 }
 
 

@@ -7,6 +7,7 @@
 #include <string>
 
 #include "pm_photonmap.cuh"
+#include "pm_scene.cuh"
 
 namespace pm {
 
@@ -36,6 +37,20 @@ struct DevMap {
   }
 };
 
+struct DevScene {
+  int64_t n_faces = 0;
+  int n_lights = 0;
+  DevBuf tri, nrm, geo, mat, lights, mt, nodes, verts_in, nrms_in;
+  bool built = false;
+  void release() {
+    tri.release(); nrm.release(); geo.release(); mat.release();
+    lights.release(); mt.release(); nodes.release();
+    verts_in.release(); nrms_in.release();
+    built = false;
+    n_faces = 0;
+  }
+};
+
 // Work counters: each kNN launch takes the next slot of a ring, so launches
 // in flight on different streams do not share a counter (up to kCounterRing
 // launches in flight at once).
@@ -50,6 +65,10 @@ struct pm_ctx {
   std::mutex mu;
   std::string err;
   pm::DevMap maps[2];
+  int64_t map_emitted[2] = {0, 0};  // photons emitted for each traced map
+  pm::DevScene scene;
+  pm::DevBuf dev_err;   // device error word of the kernels (int)
+  pm::DevBuf trace_raw, trace_keys, trace_misc;  // photon tracing buffers
   pm::DevBuf scratch;  // map build scratch
   pm::DevBuf q_in, q_out;  // staging of the host-pointer entry points
   pm::DevBuf counter;      // kCounterRing work counters
@@ -72,6 +91,25 @@ struct pm_ctx {
     q_out.release();
     counter.release();
     stats.release();
+    scene.release();
+    dev_err.release();
+    trace_raw.release();
+    trace_keys.release();
+    trace_misc.release();
+  }
+  pm::SceneDev scene_view() const {
+    pm::SceneDev v;
+    v.tri = (const float4*)scene.tri.ptr;
+    v.nrm = (const float4*)scene.nrm.ptr;
+    v.geo = (const float4*)scene.geo.ptr;
+    v.mat = (const pm::Material*)scene.mat.ptr;
+    v.lights = (const int*)scene.lights.ptr;
+    v.mt = (const float4*)scene.mt.ptr;
+    v.nodes = (const float4*)scene.nodes.ptr;
+    v.n_faces = (int)scene.n_faces;
+    v.n_lights = scene.n_lights;
+    v.err = (int*)dev_err.ptr;
+    return v;
   }
 };
 

@@ -36,7 +36,7 @@ __global__ void __launch_bounds__(kSortThreads)
 }
 
 // Exclusive scan of m counts in place, one block of 1024 threads.
-__global__ void __launch_bounds__(1024) rs_scan(uint32_t* a, int m) {
+static __global__ void __launch_bounds__(1024) rs_scan(uint32_t* a, int m) {
   __shared__ uint32_t sums[1024];
   const int tid = threadIdx.x;
   const int per = (m + 1023) / 1024;

@@ -1,0 +1,67 @@
+"""PhotonMapping: the reference integrator's interface over the device.
+
+Mirrors ``PhotonMapping`` of integrator.h:109-570: the constructor takes the
+same six parameters, ``build`` traces the global (and, with final gathering,
+the caustics) photon map on the device, ``getPhotonMapPtr`` exposes the
+global map.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+from . import _native as N
+from ._native import Context
+from .photon_map import PhotonMap
+
+
+class TraceStats(C.Structure):
+    _fields_ = [("emitted", C.c_int64), ("stored", C.c_int64),
+                ("nan_throughput", C.c_uint32), ("negative_throughput", C.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+
+def trace_photons(ctx: Context, map_id: int, seed: int, n_emit: int, max_depth: int) -> dict:
+    """pm_photons_trace: trace n_emit photons into map `map_id`."""
+    st = TraceStats()
+    ctx.check(ctx.lib.pm_photons_trace(ctx.handle, int(map_id), C.c_uint64(seed), int(n_emit),
+                                       int(max_depth), C.addressof(st)),
+              "pm_photons_trace")
+    return st.as_dict()
+
+
+class PhotonMapping:
+    """integrator.h:380-390 constructor arguments, in order."""
+
+    def __init__(self, nPhotonsGlobal: int, nEstimationGlobal: int,
+                 nPhotonsCausticsMultiplier: float, nEstimationCaustics: int,
+                 strictCalcDepth: int, maxDepth: int, ctx: Context | None = None):
+        self.ctx = ctx if ctx is not None else Context(0)
+        self.nPhotonsGlobal = int(nPhotonsGlobal)
+        self.nEstimationGlobal = int(nEstimationGlobal)
+        # int * float, stored into an int member (integrator.h:385)
+        self.nPhotonsCaustics = int(C.c_float(nPhotonsGlobal * C.c_float(nPhotonsCausticsMultiplier).value).value)
+        self.nEstimationCaustics = int(nEstimationCaustics)
+        self.finalGatheringDepth = int(strictCalcDepth)
+        self.maxDepth = int(maxDepth)
+        self.global_map = PhotonMap(self.ctx, N.PM_MAP_GLOBAL)
+        self.caustics_map = PhotonMap(self.ctx, N.PM_MAP_CAUSTICS)
+        self.stats: dict = {}
+
+    def getPhotonMapPtr(self) -> PhotonMap:  # integrator.h:390
+        return self.global_map
+
+    def build(self, scene, seed: int = 1) -> dict:  # integrator.h:393
+        """Traces the photon maps for `scene` (already built on this
+        context). The caustics map is traced only with final gathering
+        (integrator.h:477)."""
+        self.stats = {"global": trace_photons(self.ctx, N.PM_MAP_GLOBAL, seed, self.nPhotonsGlobal,
+                                              self.maxDepth)}
+        if self.finalGatheringDepth > 0:
+            self.stats["caustics"] = trace_photons(self.ctx, N.PM_MAP_CAUSTICS, seed + 1,
+                                                   self.nPhotonsCaustics, self.maxDepth)
+        else:
+            self.ctx.check(self.ctx.lib.pm_photonmap_build(self.ctx.handle, N.PM_MAP_CAUSTICS,
+                                                           None, 0), "pm_photonmap_build")
+        return self.stats
