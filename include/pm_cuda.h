@@ -101,6 +101,11 @@ int pm_photonmap_build(pm_ctx* ctx, int map, const float* photons, int64_t n);
 int pm_photonmap_build_device(pm_ctx* ctx, int map, const void* d_photons,
                               int64_t n, void* stream);
 
+/* Sets how many photons were emitted to make `map` (nPhotonsGlobal,
+ * nPhotonsCaustics: the normalisation of integrator.h:149 and :171) for
+ * pm_render; pm_photons_trace sets it itself. */
+int pm_photonmap_set_emitted(pm_ctx* ctx, int map, int64_t n_emitted);
+
 /* PhotonMap::getNPhotons (photon_map.h:194). */
 int pm_photonmap_size(pm_ctx* ctx, int map, int64_t* n);
 
@@ -189,6 +194,57 @@ typedef struct pm_trace_stats {
  * and its order (by photon, then bounce) are reproducible. */
 int pm_photons_trace(pm_ctx* ctx, int map, uint64_t seed, int64_t n_emit,
                      int max_depth, pm_trace_stats* stats);
+
+/* -------------------------------------------------------------- render */
+/* A constructed pinhole Camera (camera.h:21-37): right = normalize(forward
+ * x (0,1,0)), up = normalize(right x forward), focal_length = 1/tan(FOV/2),
+ * computed by the caller exactly as the reference's constructor does. */
+typedef struct pm_camera {
+  float position[3];
+  float forward[3];
+  float right[3];
+  float up[3];
+  float focal_length;
+} pm_camera;
+
+typedef struct pm_render_params {
+  int32_t width, height;
+  int32_t spp;                   /* samples per pixel (n_samples)           */
+  int32_t k_global;              /* nEstimationGlobal                       */
+  int32_t k_caustics;            /* k of the caustics-map estimate; the
+                                    reference uses nEstimationGlobal there
+                                    (integrator.h:161)                       */
+  int32_t final_gathering_depth; /* strictCalcDepth                         */
+  int32_t max_depth;             /* maxDepth                                */
+  int32_t n_gather;              /* gather rays per diffuse hit at depth <
+                                    final_gathering_depth, averaged; 1 is the
+                                    reference (integrator.h:224-235)         */
+  int32_t spp_batch;             /* samples per pixel per pass, 0 = auto    */
+  int32_t reserved;
+} pm_render_params;
+
+typedef struct pm_render_stats {
+  int64_t samples;            /* camera samples taken                      */
+  int64_t dropped_nan;        /* samples dropped as NaN (main.cpp:49-52)   */
+  int64_t dropped_negative;   /* samples dropped as negative (:53-56)      */
+  int64_t queries_global;     /* global-map estimates                      */
+  int64_t queries_caustics;   /* caustics-map estimates                    */
+  int32_t passes;             /* sample batches                            */
+  int32_t reserved;
+} pm_render_stats;
+
+/* The render loop of examples/main.cpp:33-70 with
+ * PhotonMapping::integrate (integrator.h:290-377): for every pixel (i, j)
+ * a sampler seeded j + width*i takes spp samples, each a camera ray
+ * through (2(j+u)-width)/height, (2(i+v)-height)/height; NaN and negative
+ * samples are dropped but counted in the average. out_rgb receives
+ * height x width x 3 floats, row-major, divided by spp (Image::divide),
+ * before gamma correction. Uses the scene and the traced photon maps of
+ * the context; the estimates divide by the photons emitted for each map
+ * (integrator.h:149, :171). */
+int pm_render(pm_ctx* ctx, const pm_camera* camera,
+              const pm_render_params* params, float* out_rgb,
+              pm_render_stats* stats);
 
 #ifdef __cplusplus
 }

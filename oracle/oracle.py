@@ -54,6 +54,7 @@ def oracle_lib() -> C.CDLL:
             "orc_intersect": (None, [_vp, _vp, _i64, _vp]),
             "orc_trace": (_i64, [_vp, C.c_int, C.c_uint64, _i64, _i64, C.c_int, _vp, _i64, _vp]),
             "orc_sincos": (None, [_vp, _i64, _vp, _vp]),
+            "orc_render": (None, [_vp, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _vp, _vp, _vp]),
         })
     return _oracle
 
@@ -183,6 +184,21 @@ class OracleScene:
         if n > cap:
             return self.trace(map_id, seed, first, count, max_depth, cap=n)
         return out[:n], st
+
+    def render(self, global_photons, g_emitted, caustic_photons, c_emitted, camera_arr,
+               width, height, spp, k_global, k_caustics, fg_depth, max_depth, n_gather=1):
+        """Restated render loop (examples/main.cpp:33-70 + integrate)."""
+        g = _c(global_photons, np.float32).reshape(-1, 9)
+        cph = _c(caustic_photons, np.float32).reshape(-1, 9)
+        cam = _c(camera_arr, np.float32)
+        prm = np.array([width, height, spp, k_global, k_caustics, fg_depth, max_depth, n_gather],
+                       np.int32)
+        out = np.empty((height, width, 3), np.float32)
+        dropped = np.zeros(2, np.int64)
+        self.lib.orc_render(self.h, g.ctypes.data, g.shape[0], int(g_emitted), cph.ctypes.data,
+                            cph.shape[0], int(c_emitted), cam.ctypes.data, prm.ctypes.data,
+                            out.ctypes.data, dropped.ctypes.data)
+        return out, dropped
 
     def close(self):
         if self.h:

@@ -22,6 +22,7 @@
 // the argument order the reference's GCC build evaluates.
 #include <cmath>
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <vector>
 
@@ -407,6 +408,200 @@ int64_t orc_trace(void* h, int map, uint64_t seed, int64_t first, int64_t count,
 // sin and cos of n float angles with the double-precision evaluation above.
 void orc_sincos(const float* x, int64_t n, float* s, float* c) {
   for (int64_t i = 0; i < n; ++i) sincos_d(x[i], s[i], c[i]);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------ camera pass
+// Restatement of examples/main.cpp:33-70 around PhotonMapping::integrate
+// (integrator.h:133-377), recursive as in the reference. Photon-map
+// queries are exact kNN by brute force (pairs (dist2, index)), summed in
+// the reference's heap-pop order (largest pair first), in float.
+namespace orc {
+
+struct PhotonSet {
+  const float* p;
+  int64_t n;
+  int64_t emitted;
+};
+
+struct RenderCtx {
+  const Scene* s;
+  PhotonSet global, caustics;
+  int kg, kc, fg_depth, max_depth, n_gather;
+};
+
+static V estimate(const PhotonSet& pm, int k, const Surf& sf, V wo, const Mat& m) {
+  if (pm.n == 0) return mk(0, 0, 0);
+  std::vector<std::pair<float, int>> c;
+  c.reserve((size_t)pm.n);
+  for (int64_t i = 0; i < pm.n; ++i) {
+    const float* ph = pm.p + 9 * i;
+    float d2 = 0.f;
+    d2 += (sf.pos.x - ph[3]) * (sf.pos.x - ph[3]);
+    d2 += (sf.pos.y - ph[4]) * (sf.pos.y - ph[4]);
+    d2 += (sf.pos.z - ph[5]) * (sf.pos.z - ph[5]);
+    if (!std::isnan(d2)) c.push_back({d2, (int)i});
+  }
+  const size_t kk = std::min<size_t>((size_t)k, c.size());
+  std::partial_sort(c.begin(), c.begin() + kk, c.end());
+  float maxd2 = 0.f;
+  for (size_t r = 0; r < kk; ++r) maxd2 = std::max(maxd2, c[r].first);
+  V lo = mk(0, 0, 0);
+  const V wo_l = to_local(wo, sf.dpdu, sf.ns, sf.dpdv);
+  for (size_t r = kk; r-- > 0;) {
+    const float* ph = pm.p + 9 * c[r].second;
+    const V wi_l = to_local(mk(ph[6], ph[7], ph[8]), sf.dpdu, sf.ns, sf.dpdv);
+    lo = add(lo, mul(lambert_eval(m, wo_l, wi_l), mk(ph[0], ph[1], ph[2])));
+  }
+  if (kk > 0) lo = divs(lo, (float)pm.emitted * PI * maxd2);
+  return lo;
+}
+
+static V direct(const RenderCtx& c, const Surf& sf, V wo, const Mat& m, Rng& rng) {
+  const Scene& s = *c.s;
+  float pc, pp;
+  const int lf = sample_light(s, rng, pc);
+  const Surf ls = sample_point(s, lf, rng, pp);
+  const V wi = normalize(sub(ls.pos, sf.pos));
+  const float r = length(sub(ls.pos, sf.pos));
+  const float pd = pp * r * r / std::fabs(dot(neg(wi), ls.ns));
+  Hit h;
+  if (intersect(s, sf.pos, wi, RAY_EPS, r - RAY_EPS, h)) return mk(0, 0, 0);
+  const Mat& lm = s.mat[lf];
+  const V f = lambert_eval(m, to_local(wo, sf.dpdu, sf.ns, sf.dpdv),
+                           to_local(wi, sf.dpdu, sf.ns, sf.dpdv));
+  const float cs = std::fabs(dot(wi, sf.ns));
+  return divs(mul(muls(f, cs), mk(lm.le[0], lm.le[1], lm.le[2])), pc * pd);
+}
+
+static V indirect(const RenderCtx& c, V wo, const Surf& sf, const Mat& m, Rng& rng,
+                  int depth) {
+  if (depth >= c.max_depth) return mk(0, 0, 0);
+  V wil;
+  float pdf;
+  const V f = sample_bxdf(m, to_local(wo, sf.dpdu, sf.ns, sf.dpdv), 1, rng, wil, pdf);
+  const V dir = to_world(wil, sf.dpdu, sf.ns, sf.dpdv);
+  const float cs = std::fabs(dot(sf.ns, dir));
+  Hit h;
+  if (!intersect(*c.s, sf.pos, dir, RAY_EPS, 3.40282347e+38f, h)) return mk(0, 0, 0);
+  const Surf s2 = surface(*c.s, sf.pos, dir, h);
+  const Mat& m2 = c.s->mat[h.prim];
+  V x;
+  if (m2.type == 0)
+    x = estimate(c.global, c.kg, s2, neg(dir), m2);
+  else
+    x = indirect(c, neg(dir), s2, m2, rng, depth + 1);
+  return divs(mul(muls(f, cs), x), pdf);
+}
+
+static V integrate(const RenderCtx& c, V o, V d, Rng& rng, int depth) {
+  if (depth >= c.max_depth) return mk(0, 0, 0);
+  Hit h;
+  if (!intersect(*c.s, o, d, RAY_EPS, 3.40282347e+38f, h)) return mk(0, 0, 0);
+  const Surf sf = surface(*c.s, o, d, h);
+  const Mat& m = c.s->mat[h.prim];
+  if (m.le[0] > 0 || m.le[1] > 0 || m.le[2] > 0) return mk(m.le[0], m.le[1], m.le[2]);
+  const V wo = neg(d);
+  if (m.type == 0) {
+    if (depth >= c.fg_depth) return estimate(c.global, c.kg, sf, wo, m);
+    const V ld = direct(c, sf, wo, m, rng);
+    const V lc = estimate(c.caustics, c.kc, sf, wo, m);
+    V li = mk(0, 0, 0);
+    const float ig = 1.0f / (float)c.n_gather;
+    for (int g = 0; g < c.n_gather; ++g) li = add(li, muls(indirect(c, wo, sf, m, rng, 0), ig));
+    return add(add(ld, lc), li);
+  }
+  const V wo_l = to_local(wo, sf.dpdu, sf.ns, sf.dpdv);
+  if (depth >= 3) {
+    V wil;
+    float pdf;
+    const V f = sample_bxdf(m, wo_l, 1, rng, wil, pdf);
+    const V wi = to_world(wil, sf.dpdu, sf.ns, sf.dpdv);
+    const V thr = divs(muls(f, cos_term(wo, wi, sf.ns, sf.ng, 1)), pdf);
+    return mul(thr, integrate(c, sf.pos, wi, rng, depth + 1));
+  }
+  // sampleAllBxDF
+  V dirs[2], fs[2];
+  int nb = 0;
+  if (m.type == 1) {
+    dirs[0] = reflect(wo_l, mk(0, 1, 0));
+    fs[0] = divs(rho(m), std::fabs(dirs[0].y));
+    nb = 1;
+  } else {
+    float iorO, iorI;
+    V n;
+    if (wo_l.y > 0) { iorO = 1.0f; iorI = m.ior; n = mk(0, 1, 0); }
+    else { iorO = m.ior; iorI = 1.0f; n = mk(0, -1, 0); }
+    const float fr = fresnel(dot(wo_l, n), iorO, iorI);
+    dirs[0] = reflect(wo_l, n);
+    fs[0] = divs(muls(rho(m), fr), std::fabs(dirs[0].y));
+    nb = 1;
+    V tr;
+    if (refract(wo_l, n, iorO, iorI, tr)) {
+      const float sc = (iorO * iorO) / (iorI * iorI);
+      dirs[1] = tr;
+      fs[1] = divs(muls(rho(m), (1.0f - fr) * sc), std::fabs(tr.y));
+      nb = 2;
+    } else {
+      fs[0] = divs(rho(m), std::fabs(dirs[0].y));
+    }
+  }
+  V lo = mk(0, 0, 0);
+  for (int b = 0; b < nb; ++b) {
+    const V wi = to_world(dirs[b], sf.dpdu, sf.ns, sf.dpdv);
+    const V thr = muls(fs[b], std::fabs(dot(wi, sf.ns)));
+    lo = add(lo, mul(thr, integrate(c, sf.pos, wi, rng, depth + 1)));
+  }
+  return lo;
+}
+
+}  // namespace orc
+
+extern "C" {
+
+// cam: 13 floats {position, forward, right, up, focal_length};
+// iprm: {width, height, spp, k_global, k_caustics, fg_depth, max_depth,
+// n_gather}; out: height x width x 3; dropped[0..1]: NaN / negative.
+void orc_render(void* h, const float* gph, int64_t gn, int64_t g_emitted,
+                const float* cph, int64_t cn, int64_t c_emitted, const float* cam,
+                const int32_t* iprm, float* out, int64_t* dropped) {
+  RenderCtx c;
+  c.s = (const Scene*)h;
+  c.global = PhotonSet{gph, gn, g_emitted};
+  c.caustics = PhotonSet{cph, cn, c_emitted};
+  const int W = iprm[0], H = iprm[1], spp = iprm[2];
+  c.kg = iprm[3];
+  c.kc = iprm[4];
+  c.fg_depth = iprm[5];
+  c.max_depth = iprm[6];
+  c.n_gather = iprm[7];
+  const V pos = mk(cam[0], cam[1], cam[2]), fwd = mk(cam[3], cam[4], cam[5]);
+  const V right = mk(cam[6], cam[7], cam[8]), up = mk(cam[9], cam[10], cam[11]);
+  const float focal = cam[12];
+  int64_t dn = 0, dneg = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : dn, dneg)
+  for (int p = 0; p < W * H; ++p) {
+    const int i = p / W, j = p % W;
+    Rng rng{(uint64_t)(j + W * i)};
+    V acc = mk(0, 0, 0);
+    for (int k = 0; k < spp; ++k) {
+      const float u = (2.0f * (j + rng.next()) - W) / H;
+      const float v = (2.0f * (i + rng.next()) - H) / H;
+      const V pinhole = add(pos, muls(fwd, focal));
+      const V sensor = add(add(pos, muls(right, u)), muls(up, v));
+      const V rad = integrate(c, sensor, normalize(sub(pinhole, sensor)), rng, 0);
+      if (std::isnan(rad.x) || std::isnan(rad.y) || std::isnan(rad.z)) { ++dn; continue; }
+      if (rad.x < 0 || rad.y < 0 || rad.z < 0) { ++dneg; continue; }
+      acc = add(acc, rad);
+    }
+    const float k = (float)spp;
+    out[3 * p] = acc.x / k;
+    out[3 * p + 1] = acc.y / k;
+    out[3 * p + 2] = acc.z / k;
+  }
+  dropped[0] = dn;
+  dropped[1] = dneg;
 }
 
 }  // extern "C"

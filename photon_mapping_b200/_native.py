@@ -53,6 +53,7 @@ _SIGNATURES = {
     "pm_photonmap_build": (C.c_int, [_vp, C.c_int, _vp, _i64]),
     "pm_photonmap_build_device": (C.c_int, [_vp, C.c_int, _vp, _i64, _vp]),
     "pm_photonmap_size": (C.c_int, [_vp, C.c_int, C.POINTER(_i64)]),
+    "pm_photonmap_set_emitted": (C.c_int, [_vp, C.c_int, _i64]),
     "pm_photonmap_get_photons": (C.c_int, [_vp, C.c_int, _i64, _i64, _vp]),
     "pm_photonmap_knn": (C.c_int, [_vp, C.c_int, _vp, _i64, C.c_int, _vp, _vp, _vp]),
     "pm_photonmap_radiance": (C.c_int, [_vp, C.c_int, _vp, _i64, C.c_int, _i64, _vp]),
@@ -60,6 +61,7 @@ _SIGNATURES = {
     "pm_scene_upload": (C.c_int, [_vp, _vp, _vp, _vp, _i64]),
     "pm_scene_intersect": (C.c_int, [_vp, _vp, _i64, _vp]),
     "pm_photons_trace": (C.c_int, [_vp, C.c_int, C.c_uint64, _i64, C.c_int, _vp]),
+    "pm_render": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
 }
 
 

@@ -256,6 +256,16 @@ int pm_photonmap_build_device(pm_ctx* c, int map, const void* d_photons,
                    as_stream(stream));
 }
 
+int pm_photonmap_set_emitted(pm_ctx* c, int map, int64_t n_emitted) {
+  PM_CHECK_CTX(c);
+  PM_CHECK_MAP(c, map);
+  if (n_emitted < 0)
+    return set_err(c, PM_ERR_INVALID_ARGUMENT, "n_emitted %lld", (long long)n_emitted);
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->map_emitted[map] = n_emitted;
+  return PM_OK;
+}
+
 int pm_photonmap_size(pm_ctx* c, int map, int64_t* n) {
   PM_CHECK_CTX(c);
   PM_CHECK_MAP(c, map);

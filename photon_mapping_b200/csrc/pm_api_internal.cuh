@@ -40,6 +40,8 @@ struct DevMap {
 struct DevScene {
   int64_t n_faces = 0;
   int n_lights = 0;
+  bool has_specular = false;
+  float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // bounds of the vertices
   DevBuf tri, nrm, geo, mat, lights, mt, nodes, verts_in, nrms_in;
   bool built = false;
   void release() {
@@ -69,6 +71,7 @@ struct pm_ctx {
   pm::DevScene scene;
   pm::DevBuf dev_err;   // device error word of the kernels (int)
   pm::DevBuf trace_raw, trace_keys, trace_misc;  // photon tracing buffers
+  pm::DevBuf r_rng, r_accum, r_slots, r_srec, r_res, r_sort, r_misc;  // render
   pm::DevBuf scratch;  // map build scratch
   pm::DevBuf q_in, q_out;  // staging of the host-pointer entry points
   pm::DevBuf counter;      // kCounterRing work counters
@@ -96,6 +99,8 @@ struct pm_ctx {
     trace_raw.release();
     trace_keys.release();
     trace_misc.release();
+    r_rng.release(); r_accum.release(); r_slots.release(); r_srec.release();
+    r_res.release(); r_sort.release(); r_misc.release();
   }
   pm::SceneDev scene_view() const {
     pm::SceneDev v;

@@ -1,0 +1,148 @@
+// C ABI of the camera pass (pm_render).
+#include "../../include/pm_cuda.h"
+#include "pm_api_internal.cuh"
+#include "pm_render.cuh"
+#include "pm_sort.cuh"
+
+using namespace pm;
+
+static_assert(sizeof(pm_camera) == 13 * 4, "camera layout");
+
+extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
+                         const pm_render_params* prm, float* out_rgb,
+                         pm_render_stats* stats) {
+  if (!c) return PM_ERR_INVALID_ARGUMENT;
+  if (!cam || !prm || !out_rgb)
+    return set_err(c, PM_ERR_INVALID_ARGUMENT, "camera / params / output");
+  const pm_render_params p = *prm;
+  if (p.width <= 0 || p.height <= 0 || (int64_t)p.width * p.height > (1 << 26) ||
+      p.spp < 0 || p.max_depth < 0 || p.n_gather < 1 || p.n_gather > 64 ||
+      p.k_global < 1 || p.k_global > PM_MAX_K || p.k_caustics < 1 ||
+      p.k_caustics > PM_MAX_K || p.spp_batch < 0)
+    return set_err(c, PM_ERR_INVALID_ARGUMENT, "render parameters");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (!c->scene.built) return set_err(c, PM_ERR_NOT_BUILT, "scene not built");
+  if (!c->maps[0].built) return set_err(c, PM_ERR_NOT_BUILT, "global photon map not built");
+  const bool need_caustics = p.final_gathering_depth > 0;
+  if (need_caustics && !c->maps[1].built)
+    return set_err(c, PM_ERR_NOT_BUILT, "caustics photon map not built");
+  cudaStream_t st = c->stream;
+  const int npix = p.width * p.height;
+  // query slots per sample: every diffuse leaf of the path tree (at most 8
+  // with specular branching) needs 1 estimate, or 1 + n_gather with final
+  // gathering
+  const int per_leaf = need_caustics ? 1 + p.n_gather : 1;
+  const int q_per_sample = (c->scene.has_specular ? 8 : 1) * per_leaf;
+  int batch = p.spp_batch;
+  if (batch <= 0) {
+    const int64_t budget = (int64_t)32 << 20;  // slots per pass
+    batch = (int)std::max<int64_t>(1, budget / ((int64_t)npix * q_per_sample));
+  }
+  batch = std::max(1, std::min(batch, std::max(p.spp, 1)));
+  const int64_t n_samples = (int64_t)npix * batch;
+  const int64_t n_slots = n_samples * q_per_sample;
+  if (n_slots > 0x7fffffffLL)
+    return set_err(c, PM_ERR_INVALID_ARGUMENT, "too many query slots per pass");
+  int s;
+  if ((s = c->r_rng.ensure((size_t)npix * 8)) || (s = c->r_accum.ensure((size_t)npix * 16)) ||
+      (s = c->r_slots.ensure((size_t)n_slots * 64)) ||
+      (s = c->r_srec.ensure((size_t)n_samples * 16)) ||
+      (s = c->r_res.ensure((size_t)n_slots * 12)) ||
+      (s = c->r_sort.ensure((size_t)n_slots * 16 + 256 * (size_t)sort_tiles(n_slots) * 4 + 64)) ||
+      (s = c->r_misc.ensure(64)) ||
+      (s = c->dev_err.ensure(64)) || (s = c->q_out.ensure((size_t)npix * 12)))
+    return set_err(c, s, "render buffers (%lld query slots)", (long long)n_slots);
+  cudaError_t e;
+  unsigned long long* dropped = (unsigned long long*)c->r_misc.ptr;
+  unsigned* qcount = (unsigned*)((char*)c->r_misc.ptr + 16);
+  if ((e = cudaMemsetAsync(c->r_accum.ptr, 0, (size_t)npix * 16, st)) ||
+      (e = cudaMemsetAsync(c->r_misc.ptr, 0, 64, st)) ||
+      (e = cudaMemsetAsync(c->dev_err.ptr, 0, 64, st)))
+    return cuda_status(c, e, "render init");
+  render_rng_init((unsigned long long*)c->r_rng.ptr, p.width, p.height, st);
+
+  RenderArgs a;
+  a.cam_pos = v3(cam->position[0], cam->position[1], cam->position[2]);
+  a.cam_fwd = v3(cam->forward[0], cam->forward[1], cam->forward[2]);
+  a.cam_right = v3(cam->right[0], cam->right[1], cam->right[2]);
+  a.cam_up = v3(cam->up[0], cam->up[1], cam->up[2]);
+  a.focal = cam->focal_length;
+  a.width = p.width;
+  a.height = p.height;
+  a.q_per_sample = q_per_sample;
+  a.fg_depth = p.final_gathering_depth;
+  a.max_depth = p.max_depth;
+  a.n_gather = p.n_gather;
+  const float ig = 1.0f / (float)p.n_gather;
+  a.inv_gather = v3(ig, ig, ig);
+  a.rng_state = (unsigned long long*)c->r_rng.ptr;
+  a.slots = (float4*)c->r_slots.ptr;
+  a.sample_rec = (float4*)c->r_srec.ptr;
+  a.err = (int*)c->dev_err.ptr;
+  const SceneDev sv = c->scene_view();
+
+  uint32_t* ka = (uint32_t*)c->r_sort.ptr;
+  uint32_t* kb = ka + n_slots;
+  uint32_t* va = kb + n_slots;
+  uint32_t* vb = va + n_slots;
+  uint32_t* hist = vb + n_slots;
+  int64_t q_tot[2] = {0, 0};
+  int passes = 0;
+  for (int done = 0; done < p.spp; done += batch) {
+    const int b = std::min(batch, p.spp - done);
+    a.batch = b;
+    const int64_t ns = (int64_t)npix * b;
+    render_camera(sv, a, st);
+    for (int map = 0; map < 2; ++map) {
+      if (map == 1 && !need_caustics) continue;
+      if ((e = cudaMemsetAsync(qcount, 0, 4, st)) != cudaSuccess)
+        return cuda_status(c, e, "render");
+      render_list_queries(a.slots, a.sample_rec, ns, q_per_sample, map,
+                          c->scene.lo, c->scene.hi, ka, va, qcount, st);
+      unsigned nq = 0;
+      if ((e = cudaMemcpyAsync(&nq, qcount, 4, cudaMemcpyDeviceToHost, st)) ||
+          (e = cudaStreamSynchronize(st)))
+        return cuda_status(c, e, "render queries");
+      q_tot[map] += nq;
+      if (nq == 0) continue;
+      const bool in_b = radix_sort_pairs<uint32_t>(ka, va, kb, vb, (int)nq, 30, hist, st);
+      KnnOut o{};
+      o.rgb = (float*)c->r_res.ptr;
+      o.stats = c->stats_ptr();
+      const int k = map == 0 ? p.k_global : p.k_caustics;
+      e = knn_launch(map_view(c->maps[map]), a.slots, nq, k, kModeRadiance,
+                     (float)c->map_emitted[map], o, c->next_counter(), c->num_sms, st,
+                     in_b ? vb : va, 4);
+      if (e != cudaSuccess) return cuda_status(c, e, "render estimates");
+    }
+    render_resolve(a.slots, a.sample_rec, (const float*)c->r_res.ptr, npix, b,
+                   q_per_sample, (float4*)c->r_accum.ptr, dropped, st);
+    ++passes;
+  }
+  render_finish((const float4*)c->r_accum.ptr, npix, std::max(p.spp, 1),
+                (float*)c->q_out.ptr, st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(c, e, "render");
+  unsigned long long hd[2] = {0, 0};
+  int herr = 0;
+  if ((e = cudaMemcpyAsync(out_rgb, c->q_out.ptr, (size_t)npix * 12,
+                           cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaMemcpyAsync(hd, dropped, 16, cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaMemcpyAsync(&herr, c->dev_err.ptr, 4, cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaStreamSynchronize(st)))
+    return cuda_status(c, e, "render output");
+  if (herr) {
+    cudaMemsetAsync(c->dev_err.ptr, 0, 4, st);
+    return set_err(c, PM_ERR_DEVICE_STATUS, "render: device error bits 0x%x", herr);
+  }
+  if (stats) {
+    stats->samples = (int64_t)npix * p.spp;
+    stats->dropped_nan = (int64_t)hd[0];
+    stats->dropped_negative = (int64_t)hd[1];
+    stats->queries_global = q_tot[0];
+    stats->queries_caustics = q_tot[1];
+    stats->passes = passes;
+    stats->reserved = 0;
+  }
+  return PM_OK;
+}

@@ -71,6 +71,20 @@ int pm_scene_upload(pm_ctx* c, const float* vertices, const float* normals,
       lights.push_back((int)f);
   sc.n_faces = n;
   sc.n_lights = (int)lights.size();
+  sc.has_specular = false;
+  for (int a = 0; a < 3; ++a) {
+    sc.lo[a] = n > 0 ? vertices[a] : 0.f;
+    sc.hi[a] = sc.lo[a];
+  }
+  for (int64_t f = 0; f < n; ++f) {
+    sc.has_specular |= materials[f].type != PM_LAMBERT;
+    for (int k = 0; k < 3; ++k)
+      for (int a = 0; a < 3; ++a) {
+        const float x = vertices[9 * f + 3 * k + a];
+        if (x < sc.lo[a]) sc.lo[a] = x;
+        if (x > sc.hi[a]) sc.hi[a] = x;
+      }
+  }
   if (n == 0) {
     sc.built = true;
     return PM_OK;

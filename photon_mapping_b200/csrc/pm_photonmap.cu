@@ -716,7 +716,8 @@ template <int C, int MODE, bool S>
 __global__ void __launch_bounds__(256, 4)
     knn_kernel(MapDev m, const void* __restrict__ queries, int64_t nq, int k,
                float n_emitted, KnnOut out,
-               unsigned long long* __restrict__ counter) {
+               unsigned long long* __restrict__ counter,
+               const uint32_t* __restrict__ order, int stride4) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ Levels L;
   WarpBuf<C>& s = reinterpret_cast<WarpBuf<C>*>(smem_raw)[threadIdx.x >> 5];
@@ -747,10 +748,12 @@ __global__ void __launch_bounds__(256, 4)
       q.k = k;
       q.cnt = 0;
       q.tau = kInf;
+      const int64_t rec = (MODE == kModeRadiance && order) ? (int64_t)__ldg(order + qi) : qi;
       if (MODE == kModeRadiance) {
         // radiance record r0 = {pos, rho.r}; wo, ns and the other albedo
         // channels are read after the search
-        const float4 r0 = __ldg(reinterpret_cast<const float4*>(queries) + 3 * qi);
+        const float4 r0 =
+            __ldg(reinterpret_cast<const float4*>(queries) + stride4 * rec);
         q.x = r0.x; q.y = r0.y; q.z = r0.z;
       } else {
         const float* q3 = reinterpret_cast<const float*>(queries) + 3 * qi;
@@ -798,7 +801,8 @@ __global__ void __launch_bounds__(256, 4)
 
       if (MODE == kModeRadiance) {
         // r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b}
-        const float4* q4 = reinterpret_cast<const float4*>(queries) + 3 * qi;
+        const float4* q4 =
+            reinterpret_cast<const float4*>(queries) + stride4 * rec;
         const float4 r0 = __ldg(q4);
         const float4 r1 = __ldg(q4 + 1);
         const float4 r2 = __ldg(q4 + 2);
@@ -806,11 +810,13 @@ __global__ void __launch_bounds__(256, 4)
         const float fr = __fdiv_rn(r0.w, kPI);
         const float fg = __fdiv_rn(r1.w, kPI);
         const float fb = __fdiv_rn(r2.w, kPI);
+        // the kept entries, in the walk's order whatever the bound was, so
+        // the sum below does not depend on the order queries are answered
+        const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
         float lr = 0.f, lg = 0.f, lb = 0.f;
-        for (int i = lane; i < cnt; i += 32) {
-          const uint32_t key = s.key[i];
+        for (int i = lane; i < nk; i += 32) {
           const uint32_t id = s.id[i];
-          if (all || keep_entry(m.pos4, key, id, kth_key, kth_oid)) {
+          {
             const float4 t = __ldg(m.thr4 + id);
             const float2 w = __ldg(m.wi2 + id);
             const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
@@ -835,9 +841,9 @@ __global__ void __launch_bounds__(256, 4)
             o3 = make_float3(__fdiv_rn(lr, den), __fdiv_rn(lg, den),
                              __fdiv_rn(lb, den));
           }
-          out.rgb[3 * qi + 0] = o3.x;
-          out.rgb[3 * qi + 1] = o3.y;
-          out.rgb[3 * qi + 2] = o3.z;
+          out.rgb[3 * rec + 0] = o3.x;
+          out.rgb[3 * rec + 1] = o3.y;
+          out.rgb[3 * rec + 2] = o3.z;
         }
       } else {
         int n2 = cnt;
@@ -886,7 +892,8 @@ template <int C, int MODE>
 static cudaError_t launch_one(const MapDev& m, const void* queries,
                               int64_t nq, int k, float n_emitted, KnnOut out,
                               unsigned long long* counter, int num_sms,
-                              cudaStream_t st) {
+                              cudaStream_t st, const uint32_t* order,
+                              int stride4) {
   constexpr int kThreads = (C <= 512) ? 256 : 128;
   const size_t smem = (kThreads / 32) * sizeof(WarpBuf<C>);
   auto kern = out.stats ? knn_kernel<C, MODE, true> : knn_kernel<C, MODE, false>;
@@ -907,27 +914,27 @@ static cudaError_t launch_one(const MapDev& m, const void* queries,
   e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
   kern<<<(unsigned)blocks, kThreads, smem, st>>>(m, queries, nq, k, n_emitted,
-                                                 out, counter);
+                                                 out, counter, order, stride4);
   return cudaGetLastError();
 }
 
 cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                        int k, int mode, float n_emitted, KnnOut out,
                        unsigned long long* counter, int num_sms,
-                       cudaStream_t st) {
+                       cudaStream_t st, const uint32_t* order, int stride4) {
   if (nq <= 0) return cudaSuccess;
   if (k <= 224) {
     return mode == kModeRadiance
                ? launch_one<512, kModeRadiance>(m, queries, nq, k, n_emitted,
-                                                out, counter, num_sms, st)
+                                                out, counter, num_sms, st, order, stride4)
                : launch_one<512, kModeKnn>(m, queries, nq, k, n_emitted, out,
-                                           counter, num_sms, st);
+                                           counter, num_sms, st, order, stride4);
   }
   return mode == kModeRadiance
              ? launch_one<2048, kModeRadiance>(m, queries, nq, k, n_emitted,
-                                               out, counter, num_sms, st)
+                                               out, counter, num_sms, st, order, stride4)
              : launch_one<2048, kModeKnn>(m, queries, nq, k, n_emitted, out,
-                                          counter, num_sms, st);
+                                          counter, num_sms, st, order, stride4);
 }
 
 }  // namespace pm

@@ -49,7 +49,7 @@ void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
 enum KnnMode { kModeRadiance = 0, kModeKnn = 1 };
 
 struct KnnOut {
-  float* rgb;          // radiance mode: 3 floats per query
+  float* rgb;          // radiance mode: 3 floats per record
   int32_t* idx;        // knn mode: k per query
   int32_t* count;      // knn mode
   float* maxd2;        // knn mode
@@ -57,12 +57,15 @@ struct KnnOut {
 };
 
 // Launches the warp-per-query k-nearest-neighbour kernel.
-//   radiance mode: queries = pm_radiance_query records (3 float4 each)
-//   knn mode:      queries = 3 floats per query
+//   radiance mode: query i reads the record r = order ? order[i] : i, a
+//                  pm_radiance_query at queries + stride4 * r float4s, and
+//                  writes rgb[3r .. 3r+3)
+//   knn mode:      queries = 3 floats per query (order and stride unused)
 // `counter` is one device word of scratch (reset by this call).
 cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                        int k, int mode, float n_emitted, KnnOut out,
                        unsigned long long* counter, int num_sms,
-                       cudaStream_t st);
+                       cudaStream_t st, const uint32_t* order = nullptr,
+                       int stride4 = 3);
 
 }  // namespace pm

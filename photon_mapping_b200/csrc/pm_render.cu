@@ -1,0 +1,324 @@
+// Camera pass of the photon mapper on the device: the render loop of
+// examples/main.cpp:33-70 around PhotonMapping::integrate
+// (integrator.h:290-377, 566-569), as a wavefront.
+//
+//   1. camera_kernel, one thread per pixel: the pixel's sampler is seeded
+//      j + width*i and draws exactly as the reference does (u and v jitter,
+//      then the integrator's draws), so sample s of a pixel sees the same
+//      random numbers as the reference's loop. The path is followed with an
+//      explicit stack (specular surfaces expand every branch at depth < 3,
+//      integrator.h:347-366, one sampled branch deeper, :326-343); light hits
+//      and next-event estimation are summed at once, every photon-map
+//      estimate the path needs (integrator.h:306-307, 310-318, 239-243) is
+//      written as a query with its path weight into the sample's slots.
+//   2. The queries of each map are sorted by the Morton code of their
+//      position and answered by the warp-per-query kNN kernel.
+//   3. resolve_kernel, one thread per pixel: per sample in order, direct +
+//      sum(weight * estimate); NaN or negative samples are dropped
+//      (main.cpp:49-56) and the rest added to the pixel.
+#include "pm_photonmap.cuh"
+#include "pm_render.cuh"
+#include "pm_scene.cuh"
+#include "pm_sort.cuh"
+
+namespace pm {
+
+constexpr int kPathStack = 8;
+
+struct Frame {
+  V3 o, d, w;
+  int depth;
+};
+
+__device__ __forceinline__ void emit_query(const RenderArgs& a, int64_t base,
+                                           int& nq, int map, const Surf& s,
+                                           V3 wo, V3 rho, V3 w) {
+  if (nq >= a.q_per_sample) {
+    atomicOr(a.err, 2);
+    return;
+  }
+  float4* r = a.slots + 4 * (base + nq);
+  r[0] = make_float4(s.pos.x, s.pos.y, s.pos.z, rho.x);
+  r[1] = make_float4(wo.x, wo.y, wo.z, rho.y);
+  r[2] = make_float4(s.ns.x, s.ns.y, s.ns.z, rho.z);
+  r[3] = make_float4(w.x, w.y, w.z, __int_as_float(map));
+  ++nq;
+}
+
+// PhotonMapping::computeDirectIllumination (integrator.h:178-213).
+__device__ V3 direct_light(const SceneDev& sc, const Surf& s, V3 wo,
+                           const Material& m, Rng& rng) {
+  float pc, pp;
+  const int lf = sample_light(sc, rng, pc);
+  const Surf ls = sample_triangle(sc, lf, rng, pp);
+  const V3 wi = normalize(ls.pos - s.pos);
+  const float r = length(ls.pos - s.pos);
+  const float pd = pp * r * r / fabsf(dot(-wi, ls.ns));
+  Hit h;
+  if (intersect(sc, s.pos, wi, kRayEps, r - kRayEps, h)) return v3(0.f, 0.f, 0.f);
+  const Material& lm = sc.mat[lf];
+  const V3 le = v3(lm.le[0], lm.le[1], lm.le[2]);
+  const V3 f = lambert_eval(m, world_to_local(wo, s.dpdu, s.ns, s.dpdv),
+                            world_to_local(wi, s.dpdu, s.ns, s.dpdv));
+  const float c = fabsf(dot(wi, s.ns));
+  return f * c * le / (pc * pd);
+}
+
+// PhotonMapping::computeIndirectIlluminationRecursive (integrator.h:
+// 215-262) for one gather ray: a diffuse hit becomes a global-map query
+// with the accumulated weight, a specular hit continues the path.
+__device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
+                       const Material* m, V3 w, Rng& rng, int64_t base,
+                       int& nq) {
+  for (int depth = 0; depth < a.max_depth; ++depth) {
+    V3 wi_l;
+    float pdf;
+    const V3 f = bxdf_sample(*m, world_to_local(wo, s.dpdu, s.ns, s.dpdv),
+                             kFromCamera, rng, wi_l, pdf);
+    const V3 dir = local_to_world(wi_l, s.dpdu, s.ns, s.dpdv);
+    const float c = fabsf(dot(s.ns, dir));
+    Hit h;
+    if (!intersect(sc, s.pos, dir, kRayEps, __int_as_float(0x7f7fffff), h)) return;
+    const Surf s2 = surface_at(sc, s.pos, dir, h);
+    const Material* m2 = sc.mat + h.prim;
+    w = w * (f * c / pdf);
+    if (m2->type == kLambert) {
+      emit_query(a, base, nq, kQueryGlobal, s2, -dir, mat_rho(*m2), w);
+      return;
+    }
+    s = s2;
+    wo = -dir;
+    m = m2;
+  }
+}
+
+__global__ void __launch_bounds__(128)
+    camera_kernel(SceneDev sc, RenderArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.width * a.height) return;
+  const int i = p / a.width, j = p % a.width;
+  Rng rng{a.rng_state[p]};
+  for (int sidx = 0; sidx < a.batch; ++sidx) {
+    const int64_t srec = (int64_t)p * a.batch + sidx;
+    const int64_t base = srec * a.q_per_sample;
+    int nq = 0;
+    V3 direct = v3(0.f, 0.f, 0.f);
+    // examples/main.cpp:40-41 and Camera::sampleRay (camera.h:41-47)
+    const float u = (2.0f * ((float)j + rng.next1d()) - (float)a.width) / (float)a.height;
+    const float v = (2.0f * ((float)i + rng.next1d()) - (float)a.height) / (float)a.height;
+    const V3 pinhole = a.cam_pos + a.focal * a.cam_fwd;
+    const V3 sensor = a.cam_pos + u * a.cam_right + v * a.cam_up;
+    Frame st[kPathStack];
+    int sp = 0;
+    st[sp++] = Frame{sensor, normalize(pinhole - sensor), v3(1.f, 1.f, 1.f), 0};
+    while (sp > 0) {
+      const Frame f = st[--sp];
+      if (f.depth >= a.max_depth) continue;
+      Hit h;
+      if (!intersect(sc, f.o, f.d, kRayEps, __int_as_float(0x7f7fffff), h)) continue;
+      const Surf s = surface_at(sc, f.o, f.d, h);
+      const Material& m = sc.mat[h.prim];
+      const V3 wo = -f.d;
+      if (m.le[0] > 0.f || m.le[1] > 0.f || m.le[2] > 0.f) {
+        direct = direct + f.w * v3(m.le[0], m.le[1], m.le[2]);
+        continue;
+      }
+      if (m.type == kLambert) {
+        if (f.depth >= a.fg_depth) {
+          emit_query(a, base, nq, kQueryGlobal, s, wo, mat_rho(m), f.w);
+        } else {
+          direct = direct + f.w * direct_light(sc, s, wo, m, rng);
+          emit_query(a, base, nq, kQueryCaustics, s, wo, mat_rho(m), f.w);
+          const V3 wg = f.w * a.inv_gather;
+          for (int g = 0; g < a.n_gather; ++g)
+            gather(a, sc, s, wo, &m, wg, rng, base, nq);
+        }
+        continue;
+      }
+      const V3 wo_l = world_to_local(wo, s.dpdu, s.ns, s.dpdv);
+      if (f.depth >= 3) {
+        V3 wi_l;
+        float pdf;
+        const V3 fb = bxdf_sample(m, wo_l, kFromCamera, rng, wi_l, pdf);
+        const V3 wi = local_to_world(wi_l, s.dpdu, s.ns, s.dpdv);
+        const V3 thr = fb * cos_term(wo, wi, s.ns, s.ng, kFromCamera) / pdf;
+        st[sp++] = Frame{s.pos, wi, f.w * thr, f.depth + 1};
+        continue;
+      }
+      // sampleAllDirection (material.h:111-118, 206-244): every branch,
+      // pushed last-first so the first one is followed first
+      V3 dir[2], fv[2];
+      int nb = 0;
+      if (m.type == kMirror) {
+        dir[0] = reflect(wo_l, v3(0.f, 1.f, 0.f));
+        fv[0] = mat_rho(m) / abs_cos_theta(dir[0]);
+        nb = 1;
+      } else {
+        float iorO, iorI;
+        V3 n;
+        if (wo_l.y > 0.f) { iorO = 1.0f; iorI = m.ior; n = v3(0.f, 1.f, 0.f); }
+        else { iorO = m.ior; iorI = 1.0f; n = v3(0.f, -1.f, 0.f); }
+        const float fr = fresnel(dot(wo_l, n), iorO, iorI);
+        dir[0] = reflect(wo_l, n);
+        fv[0] = fr * mat_rho(m) / abs_cos_theta(dir[0]);
+        nb = 1;
+        V3 tr;
+        if (refract(wo_l, n, iorO, iorI, tr)) {
+          const float scaling = (iorO * iorO) / (iorI * iorI);
+          dir[1] = tr;
+          fv[1] = (1.0f - fr) * scaling * mat_rho(m) / abs_cos_theta(tr);
+          nb = 2;
+        } else {
+          fv[0] = mat_rho(m) / abs_cos_theta(dir[0]);
+        }
+      }
+      for (int b = nb - 1; b >= 0; --b) {
+        const V3 wi = local_to_world(dir[b], s.dpdu, s.ns, s.dpdv);
+        const V3 thr = fv[b] * fabsf(dot(wi, s.ns));
+        if (sp < kPathStack) st[sp++] = Frame{s.pos, wi, f.w * thr, f.depth + 1};
+        else atomicOr(a.err, 4);
+      }
+    }
+    a.sample_rec[srec] = make_float4(direct.x, direct.y, direct.z, __int_as_float(nq));
+  }
+  a.rng_state[p] = rng.state;
+}
+
+__global__ void rng_init_kernel(unsigned long long* st, int w, int n) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const int i = p / w, j = p % w;
+  st[p] = (unsigned long long)(j + w * i);  // UniformSampler(j + width * i)
+}
+
+__device__ __forceinline__ uint32_t spread10r(uint32_t x) {
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+// Lists the slots holding a query of `map`, with the Morton code of the
+// query position (in the scene box) as the sort key.
+__global__ void list_queries_kernel(const float4* __restrict__ slots,
+                                    const float4* __restrict__ srec,
+                                    int64_t n_samples, int q_per_sample, int map,
+                                    float3 lo, float3 inv_ext,
+                                    uint32_t* __restrict__ keys,
+                                    uint32_t* __restrict__ vals,
+                                    unsigned* __restrict__ count) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  // every lane reaches the ballot and the shuffle (no early exit)
+  bool mine = false;
+  float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (t < n_samples * q_per_sample) {
+    const int64_t sidx = t / q_per_sample;
+    const int q = (int)(t % q_per_sample);
+    if (q < __float_as_int(srec[sidx].w)) {
+      mine = __float_as_int(slots[4 * t + 3].w) == map;
+      r0 = slots[4 * t];
+    }
+  }
+  const unsigned bal = __ballot_sync(kFull, mine);
+  unsigned base = 0;
+  const int leader = bal ? __ffs(bal) - 1 : 0;
+  if (bal && (int)lane_id() == leader)
+    base = atomicAdd(count, (unsigned)__popc(bal));
+  base = __shfl_sync(kFull, base, leader);
+  if (!mine) return;
+  const unsigned o = base + __popc(bal & lanemask_lt());
+  auto cell = [](float v, float l, float ie) -> uint32_t {
+    const float c = (v - l) * ie * 1024.f;
+    if (!(c > 0.f)) return 0u;
+    return c >= 1023.f ? 1023u : (uint32_t)c;
+  };
+  keys[o] = (spread10r(cell(r0.x, lo.x, inv_ext.x)) << 2) |
+            (spread10r(cell(r0.y, lo.y, inv_ext.y)) << 1) |
+            spread10r(cell(r0.z, lo.z, inv_ext.z));
+  vals[o] = (uint32_t)t;
+}
+
+__global__ void resolve_kernel(const float4* __restrict__ slots,
+                               const float4* __restrict__ srec,
+                               const float* __restrict__ res, int npix,
+                               int batch, int q_per_sample,
+                               float4* __restrict__ accum,
+                               unsigned long long* __restrict__ dropped) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npix) return;
+  float4 acc = accum[p];
+  unsigned nan_n = 0, neg_n = 0;
+  for (int s = 0; s < batch; ++s) {
+    const int64_t sidx = (int64_t)p * batch + s;
+    const float4 d = srec[sidx];
+    V3 rad = v3(d.x, d.y, d.z);
+    const int nq = __float_as_int(d.w);
+    for (int q = 0; q < nq; ++q) {
+      const int64_t t = sidx * q_per_sample + q;
+      const float4 w = slots[4 * t + 3];
+      const V3 l = v3(res[3 * t], res[3 * t + 1], res[3 * t + 2]);
+      rad = rad + v3(w.x, w.y, w.z) * l;
+    }
+    if (has_nan(rad)) { ++nan_n; continue; }
+    if (rad.x < 0.f || rad.y < 0.f || rad.z < 0.f) { ++neg_n; continue; }
+    acc.x += rad.x;
+    acc.y += rad.y;
+    acc.z += rad.z;
+  }
+  accum[p] = acc;
+  if (nan_n) atomicAdd(dropped, (unsigned long long)nan_n);
+  if (neg_n) atomicAdd(dropped + 1, (unsigned long long)neg_n);
+}
+
+__global__ void finish_kernel(const float4* __restrict__ accum, int npix,
+                              float spp, float* __restrict__ out) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= npix) return;
+  const float4 a = accum[p];
+  // Image::divide (image.h:49-56)
+  out[3 * p] = a.x / spp;
+  out[3 * p + 1] = a.y / spp;
+  out[3 * p + 2] = a.z / spp;
+}
+
+void render_rng_init(unsigned long long* st, int w, int h, cudaStream_t s) {
+  const int n = w * h;
+  rng_init_kernel<<<(n + 255) / 256, 256, 0, s>>>(st, w, n);
+}
+
+void render_camera(const SceneDev& sc, const RenderArgs& a, cudaStream_t s) {
+  const int n = a.width * a.height;
+  camera_kernel<<<(n + 127) / 128, 128, 0, s>>>(sc, a);
+}
+
+void render_list_queries(const float4* slots, const float4* srec,
+                         int64_t n_samples, int q_per_sample, int map,
+                         const float* scene_lo, const float* scene_hi,
+                         uint32_t* keys, uint32_t* vals, unsigned* count,
+                         cudaStream_t s) {
+  const int64_t n = n_samples * q_per_sample;
+  if (n <= 0) return;
+  float3 lo = make_float3(scene_lo[0], scene_lo[1], scene_lo[2]);
+  float3 ie;
+  ie.x = scene_hi[0] > scene_lo[0] ? 1.0f / (scene_hi[0] - scene_lo[0]) : 0.f;
+  ie.y = scene_hi[1] > scene_lo[1] ? 1.0f / (scene_hi[1] - scene_lo[1]) : 0.f;
+  ie.z = scene_hi[2] > scene_lo[2] ? 1.0f / (scene_hi[2] - scene_lo[2]) : 0.f;
+  list_queries_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(
+      slots, srec, n_samples, q_per_sample, map, lo, ie, keys, vals, count);
+}
+
+void render_resolve(const float4* slots, const float4* srec, const float* res,
+                    int npix, int batch, int q_per_sample, float4* accum,
+                    unsigned long long* dropped, cudaStream_t s) {
+  resolve_kernel<<<(npix + 127) / 128, 128, 0, s>>>(
+      slots, srec, res, npix, batch, q_per_sample, accum, dropped);
+}
+
+void render_finish(const float4* accum, int npix, int spp, float* out,
+                   cudaStream_t s) {
+  finish_kernel<<<(npix + 255) / 256, 256, 0, s>>>(accum, npix, (float)spp, out);
+}
+
+}  // namespace pm

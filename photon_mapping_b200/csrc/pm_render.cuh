@@ -1,0 +1,39 @@
+// Camera-pass launchers (see pm_render.cu).
+#pragma once
+
+#include "pm_scene.cuh"
+
+namespace pm {
+
+enum { kQueryGlobal = 0, kQueryCaustics = 1 };
+
+struct RenderArgs {
+  V3 cam_pos, cam_fwd, cam_right, cam_up;
+  float focal;
+  int width, height;
+  int batch;         // samples per pixel in this pass
+  int q_per_sample;  // query slots per sample
+  int fg_depth;      // finalGatheringDepth
+  int max_depth;
+  int n_gather;      // gather rays per diffuse hit (1 in the reference)
+  V3 inv_gather;     // 1 / n_gather
+  unsigned long long* rng_state;  // per pixel, kept across passes
+  float4* slots;       // 4 float4 per query slot
+  float4* sample_rec;  // per sample {direct radiance, query count bits}
+  int* err;            // bit 1: slots exhausted, bit 2: path stack full
+};
+
+void render_rng_init(unsigned long long* st, int w, int h, cudaStream_t s);
+void render_camera(const SceneDev& sc, const RenderArgs& a, cudaStream_t s);
+void render_list_queries(const float4* slots, const float4* srec,
+                         int64_t n_samples, int q_per_sample, int map,
+                         const float* scene_lo, const float* scene_hi,
+                         uint32_t* keys, uint32_t* vals, unsigned* count,
+                         cudaStream_t s);
+void render_resolve(const float4* slots, const float4* srec, const float* res,
+                    int npix, int batch, int q_per_sample, float4* accum,
+                    unsigned long long* dropped, cudaStream_t s);
+void render_finish(const float4* accum, int npix, int spp, float* out,
+                   cudaStream_t s);
+
+}  // namespace pm

@@ -14,6 +14,22 @@ from ._native import Context
 from .photon_map import PhotonMap
 
 
+class RenderParams(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
+                ("k_global", C.c_int32), ("k_caustics", C.c_int32),
+                ("final_gathering_depth", C.c_int32), ("max_depth", C.c_int32),
+                ("n_gather", C.c_int32), ("spp_batch", C.c_int32), ("reserved", C.c_int32)]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("samples", C.c_int64), ("dropped_nan", C.c_int64),
+                ("dropped_negative", C.c_int64), ("queries_global", C.c_int64),
+                ("queries_caustics", C.c_int64), ("passes", C.c_int32), ("reserved", C.c_int32)]
+
+    def as_dict(self) -> dict:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
+
+
 class TraceStats(C.Structure):
     _fields_ = [("emitted", C.c_int64), ("stored", C.c_int64),
                 ("nan_throughput", C.c_uint32), ("negative_throughput", C.c_uint32)]
@@ -65,3 +81,20 @@ class PhotonMapping:
             self.ctx.check(self.ctx.lib.pm_photonmap_build(self.ctx.handle, N.PM_MAP_CAUSTICS,
                                                            None, 0), "pm_photonmap_build")
         return self.stats
+
+    def render(self, camera, width: int, height: int, n_samples: int, n_gather: int = 1,
+               spp_batch: int = 0):
+        """The render loop of examples/main.cpp:33-70 on the device: returns
+        (image (height, width, 3) float32 averaged over n_samples, stats).
+        The caustics estimate uses k = nEstimationGlobal like the reference
+        (integrator.h:161)."""
+        import numpy as np
+        p = RenderParams(int(width), int(height), int(n_samples), self.nEstimationGlobal,
+                         self.nEstimationGlobal, self.finalGatheringDepth, self.maxDepth,
+                         int(n_gather), int(spp_batch), 0)
+        out = np.empty((height, width, 3), np.float32)
+        st = RenderStats()
+        cam = camera.as_struct()
+        self.ctx.check(self.ctx.lib.pm_render(self.ctx.handle, C.addressof(cam), C.addressof(p),
+                                              out.ctypes.data, C.addressof(st)), "pm_render")
+        return out, st.as_dict()

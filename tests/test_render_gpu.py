@@ -1,0 +1,86 @@
+"""Parity of the device camera pass (pm_render) with the oracle's
+restatement of the reference's render loop and integrator.
+
+Both take the same traced photon maps and the same per-pixel random
+streams, so the control flow is identical; images agree per pixel up to
+the order of float sums (tolerance below).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from photon_mapping_b200 import scene as S
+from photon_mapping_b200.camera import Camera
+from photon_mapping_b200.integrator import PhotonMapping
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 2e-5   # per pixel and channel, relative (float sum order only)
+ATOL = 1e-6
+
+
+def setup(ctx, mesh, n_photons, k, fg_depth, max_depth, mult=1.0, seed=3):
+    sc = S.Scene(ctx)
+    sc.setMesh(mesh)
+    sc.build()
+    pmi = PhotonMapping(n_photons, k, mult, k, fg_depth, max_depth, ctx=ctx)
+    pmi.build(sc, seed=seed)
+    return pmi
+
+
+def oracle_render(mesh, pmi, cam, w, h, spp, n_gather=1):
+    g = pmi.global_map.photons()
+    c = pmi.caustics_map.photons()
+    return O.OracleScene(mesh).render(g, pmi.nPhotonsGlobal, c, pmi.nPhotonsCaustics,
+                                      cam.as_array(), w, h, spp, pmi.nEstimationGlobal,
+                                      pmi.nEstimationGlobal, pmi.finalGatheringDepth,
+                                      pmi.maxDepth, n_gather)
+
+
+def assert_images_close(got, want):
+    np.testing.assert_array_equal(np.isfinite(got), np.isfinite(want))
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=ATOL)
+
+
+def test_cornell_no_final_gathering(ctx):
+    mesh = S.cornell_box(0)
+    pmi = setup(ctx, mesh, 20000, 50, 0, 100)
+    cam = Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
+    img, st = pmi.render(cam, 40, 32, 3)
+    want, dropped = oracle_render(mesh, pmi, cam, 40, 32, 3)
+    assert_images_close(img, want)
+    assert st["dropped_nan"] == dropped[0] and st["dropped_negative"] == dropped[1]
+    assert st["queries_caustics"] == 0 and st["queries_global"] > 0
+    assert img.mean() > 0
+
+
+def test_cornell_final_gathering(ctx):
+    mesh = S.cornell_box(1)
+    pmi = setup(ctx, mesh, 20000, 40, 1, 20)
+    cam = Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
+    img, st = pmi.render(cam, 24, 24, 2, spp_batch=1)
+    want, dropped = oracle_render(mesh, pmi, cam, 24, 24, 2)
+    assert_images_close(img, want)
+    assert st["passes"] == 2
+
+
+def test_caustics_scene_specular_branches(ctx):
+    mesh = S.caustics_scene(0, grid=24, subdiv=2)
+    pmi = setup(ctx, mesh, 20000, 30, 1, 12, mult=2.0)
+    assert pmi.caustics_map.getNPhotons() > 0
+    cam = Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
+    img, st = pmi.render(cam, 24, 20, 2)
+    want, dropped = oracle_render(mesh, pmi, cam, 24, 20, 2)
+    assert_images_close(img, want)
+    assert st["queries_caustics"] > 0
+
+
+def test_multiple_gather_rays(ctx):
+    mesh = S.cornell_box(2)
+    pmi = setup(ctx, mesh, 10000, 20, 1, 10)
+    cam = Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
+    img, st = pmi.render(cam, 16, 16, 2, n_gather=4)
+    want, _ = oracle_render(mesh, pmi, cam, 16, 16, 2, n_gather=4)
+    np.testing.assert_allclose(img, want, rtol=1e-4, atol=1e-6)
