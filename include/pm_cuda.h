@@ -144,6 +144,29 @@ int pm_photonmap_radiance_device(pm_ctx* ctx, int map, const void* d_queries,
                                  int64_t nq, int k, int64_t n_emitted,
                                  void* d_out_rgb, void* stream);
 
+/* ------------------------------------------- allocation-free estimate */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc
+ * (a plug-in whose host application owns all device memory and forbids
+ * allocations in its callbacks; a real-time loop that cannot afford the
+ * device-wide synchronisation of cudaMalloc/cudaFree): the radiance
+ * estimate of pm_photonmap_radiance over a photon set of at most
+ * PM_NOALLOC_MAX_PHOTONS photons, with no context and no allocation. The
+ * caller passes d_photons (n_photons x 9 floats), d_queries (16-byte
+ * aligned pm_radiance_query records) and d_out_rgb (nq x 3 floats) in
+ * device memory of the current device; the call enqueues the map build
+ * and the queries on `stream` (NULL: legacy default stream) and returns.
+ * Intermediate buffers live in one static device array (about 3.9 MiB per
+ * GPU that loads the library, kept until exit). The first call on a device
+ * looks that array's address up (cudaGetSymbolAddress) and should come
+ * before any stream capture. Calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller. Larger photon sets
+ * are rejected with PM_ERR_INVALID_ARGUMENT. */
+#define PM_NOALLOC_MAX_PHOTONS 65536
+int pm_photonmap_radiance_noalloc(const float* d_photons, int64_t n_photons,
+                                  const pm_radiance_query* d_queries,
+                                  int64_t nq, int k, int64_t n_emitted,
+                                  float* d_out_rgb, void* stream);
+
 /* --------------------------------------------------------------- scene */
 /* Per-face material, as Scene::loadModel derives it from the OBJ/MTL
  * (scene.h:15-51): illum 5 -> Mirror, illum 7 -> Glass(Ni), otherwise

@@ -24,6 +24,7 @@ PM_ERR_DEVICE_STATUS = 5
 PM_MAP_GLOBAL = 0
 PM_MAP_CAUSTICS = 1
 PM_MAX_K = 1024
+PM_NOALLOC_MAX_PHOTONS = 65536
 
 # pm_radiance_query: {px,py,pz,rho_r, wox,woy,woz,rho_g, nsx,nsy,nsz,rho_b}
 RADIANCE_QUERY_FLOATS = 12
@@ -62,6 +63,7 @@ _SIGNATURES = {
     "pm_scene_intersect": (C.c_int, [_vp, _vp, _i64, _vp]),
     "pm_photons_trace": (C.c_int, [_vp, C.c_int, C.c_uint64, _i64, C.c_int, _vp]),
     "pm_render": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "pm_photonmap_radiance_noalloc": (C.c_int, [_vp, _i64, _vp, _i64, C.c_int, _i64, _vp, _vp]),
 }
 
 
