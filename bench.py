@@ -35,9 +35,11 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 K_NEAREST = 100
-N_PHOTONS = 1 << 20
+N_EMIT = 1_000_000          # photons emitted for the global map (config 2)
+TRACE_SEED = 1
+MAX_DEPTH = 100
 IMAGE_W = IMAGE_H = 512
-SPP = 4
+SPP = 4                     # the query frame: primary hits of 512x512x4 spp
 BYTES_PER_QUERY = 36 * K_NEAREST + 24  # k photons x 36 B + position in + RGB out
 METRIC = "kNN radiance queries/s at 1M photons k=100"
 CPU_SAMPLE_QUERIES = 40000
@@ -50,23 +52,23 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-render", action="store_true", help="skip the render-rate measurements")
     return ap.parse_args()
 
 
-def workload():
-    from photon_mapping_b200 import workloads as W
-    photons = W.wall_photons(N_PHOTONS, seed=0)
-    queries = W.room_primary_hit_queries(IMAGE_W, IMAGE_H, SPP)
-    return photons, queries
+def scene_and_camera():
+    from photon_mapping_b200 import scene as S
+    from photon_mapping_b200.camera import Camera
+    return S.cornell_box(0), Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
 
 
-def config_dict(nq: int) -> dict:
+def config_dict(nq: int, n_stored: int) -> dict:
     return {
-        "workload": (f"radiance estimate k={K_NEAREST} over a {N_PHOTONS}-photon map on the walls of "
-                     f"the unit Cornell room; queries = primary hits of a {IMAGE_W}x{IMAGE_H}x{SPP}spp "
-                     "frame in pixel order"),
-        "photons": N_PHOTONS,
-        "n_emitted": N_PHOTONS,
+        "workload": (f"radiance estimate k={K_NEAREST} on the photon map traced from {N_EMIT} "
+                     f"emitted photons in the procedural Cornell box (configs[1] scene); queries = "
+                     f"primary hits of a {IMAGE_W}x{IMAGE_H}x{SPP}spp frame in pixel order"),
+        "photons_emitted": N_EMIT,
+        "photons_stored": n_stored,
         "k": K_NEAREST,
         "queries_per_step": nq,
         "l2": "flushed before every step (256 MiB device write outside the step events)",
@@ -184,11 +186,43 @@ def cpu_reference_rate(photons, queries, n_queries: int, repeats: int = 1):
     sample = np.ascontiguousarray(queries[:n_queries])
     t0 = time.perf_counter()
     for _ in range(repeats):
-        ref.radiance(sample, K_NEAREST, N_PHOTONS)
+        ref.radiance(sample, K_NEAREST, N_EMIT)
     dt = time.perf_counter() - t0
     threads = O.ref_threads()
     ref.close()
     return n_queries * repeats / dt, threads, dt
+
+
+# ---------------------------------------------------------------- render rates
+
+RENDER_CONFIGS = {
+    # 256^2, 100k photons, k=100, 16 spp, no final gathering
+    "config1": dict(width=256, height=256, spp=16, photons=100_000, k=100, fg=0, n_gather=1),
+    # 512^2, 1M photons, k=100, final gathering with 16 gather rays;
+    # timed on 2 of its 100 spp (samples/s is per sample)
+    "config2": dict(width=512, height=512, spp=2, photons=1_000_000, k=100, fg=1, n_gather=16),
+}
+
+
+def render_rates(ctx, sc, camera, dev) -> dict:
+    """Camera samples per second of pm_render (host API, wall clock) for
+    the configs above, photon maps traced beforehand."""
+    import torch
+    from photon_mapping_b200.integrator import PhotonMapping
+    out = {}
+    for name, c in RENDER_CONFIGS.items():
+        pmi = PhotonMapping(c["photons"], c["k"], 1.0, c["k"], c["fg"], MAX_DEPTH, ctx=ctx)
+        pmi.build(sc, seed=TRACE_SEED)
+        pmi.render(camera, c["width"], c["height"], 1, n_gather=c["n_gather"])  # warm-up
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        img, st = pmi.render(camera, c["width"], c["height"], c["spp"], n_gather=c["n_gather"])
+        dt = time.perf_counter() - t0
+        n = c["width"] * c["height"] * c["spp"]
+        out[name] = {"samples_per_s": n / dt, "seconds": dt, **c,
+                     "queries_global": st["queries_global"], "passes": st["passes"],
+                     "mean_radiance": float(img.mean())}
+    return out
 
 
 # -------------------------------------------------------------------- our arm
@@ -200,14 +234,26 @@ def run_ours(args) -> None:
     dist = dist_init(world, "nccl")
     dev = torch.device("cuda", local)
 
-    from photon_mapping_b200 import Context, PhotonMap
-    photons, queries = workload()
-    nq = queries.shape[0]
+    from photon_mapping_b200 import Context
+    from photon_mapping_b200 import scene as S
+    from photon_mapping_b200 import workloads as W
+    from photon_mapping_b200.integrator import PhotonMapping
+    mesh, camera = scene_and_camera()
     ctx = Context(local)
-    pm = PhotonMap(ctx)
-    pm.setPhotons(photons)
-    pm.build()
     lib = ctx.lib
+    sc = S.Scene(ctx)
+    sc.setMesh(mesh)
+    sc.build()
+    pmi = PhotonMapping(N_EMIT, K_NEAREST, 1.0, K_NEAREST, 0, MAX_DEPTH, ctx=ctx)
+    pmi.build(sc, seed=TRACE_SEED)            # warm-up trace
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    trace_stats = pmi.build(sc, seed=TRACE_SEED)["global"]
+    trace_s = time.perf_counter() - t0
+    photons = pmi.global_map.photons()
+    o, d = W.camera_rays(camera, IMAGE_W, IMAGE_H, SPP)
+    queries = W.hit_queries(mesh, o, d, sc.intersect(o, d))
+    nq = queries.shape[0]
 
     d_q = torch.from_numpy(queries).to(dev)
     d_out = torch.empty((nq, 3), dtype=torch.float32, device=dev)
@@ -217,7 +263,7 @@ def run_ours(args) -> None:
 
     def step():
         st = lib.pm_photonmap_radiance_device(ctx.handle, 0, d_q.data_ptr(), nq, K_NEAREST,
-                                              N_PHOTONS, d_out.data_ptr(), stream.cuda_stream)
+                                              N_EMIT, d_out.data_ptr(), stream.cuda_stream)
         ctx.check(st, "pm_photonmap_radiance_device")
 
     for _ in range(max(args.warmup, 0)):
@@ -255,7 +301,7 @@ def run_ours(args) -> None:
     h_out = torch.empty((nq, 3), dtype=torch.float32).pin_memory()
 
     def e2e_step():
-        st = lib.pm_photonmap_radiance(ctx.handle, 0, h_q.data_ptr(), nq, K_NEAREST, N_PHOTONS,
+        st = lib.pm_photonmap_radiance(ctx.handle, 0, h_q.data_ptr(), nq, K_NEAREST, N_EMIT,
                                        h_out.data_ptr())
         ctx.check(st, "pm_photonmap_radiance")
 
@@ -286,6 +332,8 @@ def run_ours(args) -> None:
     ctx.set_stats(False)
     per_q = {k2: v / max(st["queries"], 1) for k2, v in st.items() if k2 != "queries"}
 
+    render = {} if args.no_render else render_rates(ctx, sc, camera, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_rate(photons, queries, CPU_SAMPLE_QUERIES)
@@ -311,8 +359,8 @@ def run_ours(args) -> None:
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded photon set on the Cornell walls; primary-hit queries)",
-        "config": config_dict(nq),
+        "data": "synthetic (procedural Cornell box, seeded photon tracing and camera jitter)",
+        "config": config_dict(nq, int(photons.shape[0])),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
@@ -323,6 +371,10 @@ def run_ours(args) -> None:
                 "d2h_bytes_per_step": int(nq * 3 * 4)},
         "gpu_launches": args.steps,
         "knn_per_query": per_q,
+        "photon_trace": {"emitted": N_EMIT, "stored": trace_stats["stored"],
+                         "seconds": trace_s, "photons_per_s": N_EMIT / trace_s,
+                         "includes": "emission, tracing, ordering and the map build"},
+        "render": render,
         "clocks": clk,
         "wall_s_timed_region": t_wall,
     }
@@ -347,18 +399,23 @@ def run_reference(args) -> None:
         except Exception as e:  # pragma: no cover
             print(json.dumps({"impl": "reference", "unavailable": f"reference build failed: {e}"}))
             return
-    photons, queries = workload()
+    from photon_mapping_b200 import workloads as W
+    mesh, camera = scene_and_camera()
+    osc = O.OracleScene(mesh)
+    photons, _ = osc.trace(0, TRACE_SEED, 0, N_EMIT, MAX_DEPTH)   # same photons as the GPU trace
+    o, d = W.camera_rays(camera, IMAGE_W, IMAGE_H, SPP)
+    queries = W.hit_queries(mesh, o, d, osc.intersect(W.rays8(o, d)))
     nq = queries.shape[0]
     ref = O.RefPhotonMap(photons)
     sample = np.ascontiguousarray(queries[:CPU_SAMPLE_QUERIES // 2])
     for _ in range(max(args.warmup, 0)):
-        ref.radiance(sample[:2000], K_NEAREST, N_PHOTONS)
+        ref.radiance(sample[:2000], K_NEAREST, N_EMIT)
     times = []
     for s in range(args.steps):
         off = (s * sample.shape[0]) % max(nq - sample.shape[0], 1)
         chunk = np.ascontiguousarray(queries[off: off + sample.shape[0]])
         t0 = time.perf_counter()
-        ref.radiance(chunk, K_NEAREST, N_PHOTONS)
+        ref.radiance(chunk, K_NEAREST, N_EMIT)
         times.append(time.perf_counter() - t0)
     threads = O.ref_threads()
     ref.close()
@@ -377,8 +434,8 @@ def run_reference(args) -> None:
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded photon set on the Cornell walls; primary-hit queries)",
-        "config": config_dict(nq),
+        "data": "synthetic (procedural Cornell box, seeded photon tracing and camera jitter)",
+        "config": config_dict(nq, int(photons.shape[0])),
         "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "reference",
                          "sample": (f"{sample.shape[0]} queries per step through the reference's "
                                     "PhotonMap + radiance loop (g++ -O3 -fopenmp)")},

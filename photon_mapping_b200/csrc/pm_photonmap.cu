@@ -732,6 +732,7 @@ __global__ void __launch_bounds__(256, 4)
   }
   if (lane < 8) s.stat[lane] = 0;
   __syncthreads();
+  float r_hint = -1.f;  // last exact k-th distance this warp found
 
   while (true) {
     unsigned long long c0 = 0;
@@ -774,12 +775,38 @@ __global__ void __launch_bounds__(256, 4)
             warm = true;
           }
         }
+        // Guess and verify when no bound is known: collect with a radius a
+        // little above the last k-th distance this warp found; k photons or
+        // more inside it make the result exact, otherwise the radius
+        // doubles (twice), then the patch bound of cold_tau is used.
+        bool guess = false, need_cold = false;
+        float rg = 0.f;
         if (!warm) {
           stat_add<S>(s, lane, kStatCold, 1);
-          q.tau = cold_tau<C, S>(m.pos4, m.boxes, m.n, m.nlevels, &L, q.x, q.y,
-                              q.z, k, &s, lane);
+          if (r_hint > 0.f) {
+            guess = true;
+            rg = 1.3f * r_hint;
+            q.tau = fmaxf(rg * rg, 1e-37f);
+          } else {
+            need_cold = true;
+          }
         }
-        collect<C, S>(m, L, q, s, lane);
+        for (int attempt = 0;; ++attempt) {
+          if (need_cold) {
+            q.tau = cold_tau<C, S>(m.pos4, m.boxes, m.n, m.nlevels, &L, q.x, q.y,
+                                   q.z, k, &s, lane);
+            need_cold = false;
+            guess = false;
+          }
+          collect<C, S>(m, L, q, s, lane);
+          if (!guess || q.cnt >= k) break;
+          if (attempt < 2) {
+            rg *= 2.0f;
+            q.tau = fmaxf(rg * rg, 1e-37f);
+          } else {
+            need_cold = true;
+          }
+        }
       }
       __syncwarp();
       stat_add<S>(s, lane, kStatQueries, 1);
@@ -873,6 +900,7 @@ __global__ void __launch_bounds__(256, 4)
         have_prev = true;
         pqx = q.x; pqy = q.y; pqz = q.z;
         pkth = maxd2;
+        r_hint = sqrtf(maxd2);
       } else {
         have_prev = false;
       }

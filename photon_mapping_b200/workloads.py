@@ -189,3 +189,68 @@ def room_primary_hit_queries(width: int = 512, height: int = 512, spp: int = 4) 
     q[:, 4:7], q[:, 7] = -d[keep], rho[:, 1]
     q[:, 8:11], q[:, 11] = nrm, rho[:, 2]
     return q
+
+
+# ------------------------------------------------- traced-scene workloads
+
+def camera_rays(camera, width: int, height: int, spp: int):
+    """Camera rays of a width x height x spp frame, pixel-major and
+    sample-minor, drawn as the reference's render loop draws them
+    (examples/main.cpp:37-46, camera.h:41-47) when a sample consumes no
+    random number besides its u, v jitter (a render without final gathering
+    of a Lambert-only scene): sample s of pixel (i, j) uses draws 2s, 2s+1
+    of the sampler seeded j + width*i. Returns (origins, directions) float32."""
+    f32 = np.float32
+    ii, jj = np.meshgrid(np.arange(height), np.arange(width), indexing="ij")
+    state = (jj + width * ii).astype(np.uint64).ravel()
+    jf, if_ = jj.ravel().astype(f32), ii.ravel().astype(f32)
+    pin = (camera.position + camera.focal_length * camera.forward).astype(f32)
+    os_, ds = [], []
+    for _ in range(spp):
+        a, state = pcg32_next(state)
+        b, state = pcg32_next(state)
+        u = (f32(2.0) * (jf + pcg32_float(a)) - f32(width)) / f32(height)
+        v = (f32(2.0) * (if_ + pcg32_float(b)) - f32(height)) / f32(height)
+        sensor = ((camera.position[None, :] + u[:, None] * camera.right[None, :])
+                  + v[:, None] * camera.up[None, :]).astype(f32)
+        d = (pin[None, :] - sensor).astype(f32)
+        ln = np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+        os_.append(sensor)
+        ds.append((d / ln[:, None]).astype(f32))
+    o = np.stack(os_, axis=1).reshape(-1, 3)
+    d = np.stack(ds, axis=1).reshape(-1, 3)
+    return o, d
+
+
+def hit_queries(mesh, o, d, hits) -> np.ndarray:
+    """pm_radiance_query records for the rays whose closest hit is a
+    non-emitting Lambert face: position = o + t*d (Ray::operator()), wo =
+    -d, shading normal interpolated as triangle.h:64-71, rho of the face.
+    `hits` is (n, 4) {t, u, v, face bits} or the HIT_DTYPE records."""
+    f32 = np.float32
+    if hits.dtype.names:
+        t, u, v, prim = hits["t"], hits["u"], hits["v"], hits["prim"]
+    else:
+        t, u, v, prim = hits[:, 0], hits[:, 1], hits[:, 2], hits[:, 3].view(np.int32)
+    ok = prim >= 0
+    m = mesh.materials[np.where(ok, prim, 0)]
+    ok &= (m["type"] == 0) & ~(m["le"] > 0).any(axis=1)
+    t, u, v, prim = t[ok], u[ok], v[ok], prim[ok]
+    o, d = o[ok], d[ok]
+    pos = (o + t[:, None] * d).astype(f32)
+    n = mesh.normals[prim].reshape(-1, 3, 3)
+    w0 = (f32(1.0) - u) - v
+    ns = ((n[:, 0] * w0[:, None] + n[:, 1] * u[:, None]) + n[:, 2] * v[:, None]).astype(f32)
+    rho = mesh.materials["rho"][prim]
+    q = np.empty((pos.shape[0], 12), f32)
+    q[:, 0:3], q[:, 3] = pos, rho[:, 0]
+    q[:, 4:7], q[:, 7] = -d, rho[:, 1]
+    q[:, 8:11], q[:, 11] = ns, rho[:, 2]
+    return q
+
+
+def rays8(o, d, tmin: float = 1e-5):
+    r = np.empty((o.shape[0], 8), np.float32)
+    r[:, 0:3], r[:, 3], r[:, 4:7] = o, tmin, d
+    r[:, 7] = np.finfo(np.float32).max
+    return r
