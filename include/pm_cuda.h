@@ -269,6 +269,16 @@ int pm_render(pm_ctx* ctx, const pm_camera* camera,
               const pm_render_params* params, float* out_rgb,
               pm_render_stats* stats);
 
+/* PathTracing::integrate (integrator.h:51-106) inside the render loop of
+ * tests/test_path_tracing.cpp:25-52: spp samples per pixel from a sampler
+ * seeded j + width*i, NaN samples dropped but counted in the average.
+ * out_rgb: height x width x 3 floats, divided by spp. dropped_nan may be
+ * NULL. */
+int pm_render_path_tracing(pm_ctx* ctx, const pm_camera* camera,
+                           int32_t width, int32_t height, int32_t spp,
+                           int32_t max_depth, float* out_rgb,
+                           int64_t* dropped_nan);
+
 #ifdef __cplusplus
 }
 #endif

@@ -55,6 +55,7 @@ def oracle_lib() -> C.CDLL:
             "orc_trace": (_i64, [_vp, C.c_int, C.c_uint64, _i64, _i64, C.c_int, _vp, _i64, _vp]),
             "orc_sincos": (None, [_vp, _i64, _vp, _vp]),
             "orc_render": (None, [_vp, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _vp, _vp, _vp]),
+            "orc_render_pt": (None, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp]),
         })
     return _oracle
 
@@ -199,6 +200,14 @@ class OracleScene:
                             cph.shape[0], int(c_emitted), cam.ctypes.data, prm.ctypes.data,
                             out.ctypes.data, dropped.ctypes.data)
         return out, dropped
+
+    def render_pt(self, camera_arr, width, height, spp, max_depth):
+        cam = _c(camera_arr, np.float32)
+        out = np.empty((height, width, 3), np.float32)
+        dropped = np.zeros(1, np.int64)
+        self.lib.orc_render_pt(self.h, cam.ctypes.data, width, height, spp, max_depth,
+                               out.ctypes.data, dropped.ctypes.data)
+        return out, int(dropped[0])
 
     def close(self):
         if self.h:

@@ -605,3 +605,63 @@ void orc_render(void* h, const float* gph, int64_t gn, int64_t g_emitted,
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// PathTracing::integrate (integrator.h:60-105) in the loop of
+// tests/test_path_tracing.cpp:25-52.
+void orc_render_pt(void* h, const float* cam, int W, int H, int spp, int max_depth,
+                   float* out, int64_t* dropped) {
+  const Scene& s = *(const Scene*)h;
+  const V pos = mk(cam[0], cam[1], cam[2]), fwd = mk(cam[3], cam[4], cam[5]);
+  const V right = mk(cam[6], cam[7], cam[8]), up = mk(cam[9], cam[10], cam[11]);
+  const float focal = cam[12];
+  int64_t dn = 0;
+#pragma omp parallel for schedule(dynamic, 1) reduction(+ : dn)
+  for (int p = 0; p < W * H; ++p) {
+    const int i = p / W, j = p % W;
+    Rng rng{(uint64_t)(j + W * i)};
+    V acc = mk(0, 0, 0);
+    for (int smp = 0; smp < spp; ++smp) {
+      const float u = (2.0f * (j + rng.next()) - W) / H;
+      const float v = (2.0f * (i + rng.next()) - H) / H;
+      const V pinhole = add(pos, muls(fwd, focal));
+      const V sensor = add(add(pos, muls(right, u)), muls(up, v));
+      V o = sensor, d = normalize(sub(pinhole, sensor));
+      V rad = mk(0, 0, 0), thr = mk(1, 1, 1);
+      for (int k = 0; k < max_depth; ++k) {
+        Hit hit;
+        if (!intersect(s, o, d, RAY_EPS, 3.40282347e+38f, hit)) break;
+        const Surf sf = surface(s, o, d, hit);
+        const Mat& m = s.mat[hit.prim];
+        if (k > 0) {
+          const float q = std::min(std::max(thr.x, std::max(thr.y, thr.z)), 1.0f);
+          if (rng.next() >= q) break;
+          thr = divs(thr, q);
+        }
+        if (m.le[0] > 0 || m.le[1] > 0 || m.le[2] > 0)
+          rad = add(rad, mul(thr, mk(m.le[0], m.le[1], m.le[2])));
+        const V wo = neg(d);
+        V wil;
+        float pdf;
+        const V f = sample_bxdf(m, to_local(wo, sf.dpdu, sf.ns, sf.dpdv), 1, rng, wil, pdf);
+        const V wi = to_world(wil, sf.dpdu, sf.ns, sf.dpdv);
+        thr = mul(thr, divs(muls(f, cos_term(wo, wi, sf.ns, sf.ng, 1)), pdf));
+        o = sf.pos;
+        d = wi;
+      }
+      if (std::isnan(rad.x) || std::isnan(rad.y) || std::isnan(rad.z)) {
+        ++dn;
+        continue;
+      }
+      acc = add(acc, rad);
+    }
+    const float k = (float)(spp > 0 ? spp : 1);
+    out[3 * p] = acc.x / k;
+    out[3 * p + 1] = acc.y / k;
+    out[3 * p + 2] = acc.z / k;
+  }
+  *dropped = dn;
+}
+
+}  // extern "C"

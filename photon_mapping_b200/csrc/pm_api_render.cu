@@ -146,3 +146,51 @@ extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
   }
   return PM_OK;
 }
+
+extern "C" int pm_render_path_tracing(pm_ctx* c, const pm_camera* cam,
+                                      int32_t width, int32_t height,
+                                      int32_t spp, int32_t max_depth,
+                                      float* out_rgb, int64_t* dropped_nan) {
+  if (!c) return PM_ERR_INVALID_ARGUMENT;
+  if (!cam || !out_rgb || width <= 0 || height <= 0 ||
+      (int64_t)width * height > (1 << 26) || spp < 0 || max_depth < 0)
+    return set_err(c, PM_ERR_INVALID_ARGUMENT, "path tracing parameters");
+  std::lock_guard<std::mutex> lk(c->mu);
+  cudaSetDevice(c->device);
+  if (!c->scene.built) return set_err(c, PM_ERR_NOT_BUILT, "scene not built");
+  const int npix = width * height;
+  int s;
+  if ((s = c->q_out.ensure((size_t)npix * 12)) || (s = c->r_misc.ensure(64)) ||
+      (s = c->dev_err.ensure(64)))
+    return set_err(c, s, "path tracing buffers");
+  cudaStream_t st = c->stream;
+  cudaError_t e;
+  if ((e = cudaMemsetAsync(c->r_misc.ptr, 0, 64, st)) ||
+      (e = cudaMemsetAsync(c->dev_err.ptr, 0, 64, st)))
+    return cuda_status(c, e, "path tracing init");
+  PathArgs a;
+  a.cam_pos = v3(cam->position[0], cam->position[1], cam->position[2]);
+  a.cam_fwd = v3(cam->forward[0], cam->forward[1], cam->forward[2]);
+  a.cam_right = v3(cam->right[0], cam->right[1], cam->right[2]);
+  a.cam_up = v3(cam->up[0], cam->up[1], cam->up[2]);
+  a.focal = cam->focal_length;
+  a.width = width;
+  a.height = height;
+  a.spp = spp;
+  a.max_depth = max_depth;
+  a.out = (float*)c->q_out.ptr;
+  a.dropped = (unsigned long long*)c->r_misc.ptr;
+  render_path_tracing(c->scene_view(), a, st);
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(c, e, "path tracing");
+  unsigned long long hd = 0;
+  int herr = 0;
+  if ((e = cudaMemcpyAsync(out_rgb, c->q_out.ptr, (size_t)npix * 12,
+                           cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaMemcpyAsync(&hd, a.dropped, 8, cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaMemcpyAsync(&herr, c->dev_err.ptr, 4, cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaStreamSynchronize(st)))
+    return cuda_status(c, e, "path tracing output");
+  if (herr) return set_err(c, PM_ERR_DEVICE_STATUS, "path tracing: device error bits 0x%x", herr);
+  if (dropped_nan) *dropped_nan = (int64_t)hd;
+  return PM_OK;
+}

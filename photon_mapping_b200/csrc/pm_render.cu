@@ -322,3 +322,67 @@ void render_finish(const float4* accum, int npix, int spp, float* out,
 }
 
 }  // namespace pm
+
+namespace pm {
+
+// PathTracing::integrate (integrator.h:60-105) inside the render loop of
+// tests/test_path_tracing.cpp:25-52 (NaN samples dropped, counted in the
+// average), one thread per pixel, the pixel's sampler seeded j + width*i.
+__global__ void __launch_bounds__(128)
+    path_trace_kernel(SceneDev sc, PathArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.width * a.height) return;
+  const int i = p / a.width, j = p % a.width;
+  Rng rng{(unsigned long long)(j + a.width * i)};
+  float ax = 0.f, ay = 0.f, az = 0.f;
+  unsigned dropped = 0;
+  for (int sidx = 0; sidx < a.spp; ++sidx) {
+    const float u = (2.0f * ((float)j + rng.next1d()) - (float)a.width) / (float)a.height;
+    const float v = (2.0f * ((float)i + rng.next1d()) - (float)a.height) / (float)a.height;
+    const V3 pinhole = a.cam_pos + a.focal * a.cam_fwd;
+    const V3 sensor = a.cam_pos + u * a.cam_right + v * a.cam_up;
+    V3 o = sensor, d = normalize(pinhole - sensor);
+    V3 rad = v3(0.f, 0.f, 0.f), thr = v3(1.f, 1.f, 1.f);
+    for (int k = 0; k < a.max_depth; ++k) {
+      Hit h;
+      if (!intersect(sc, o, d, kRayEps, __int_as_float(0x7f7fffff), h)) break;
+      const Surf s = surface_at(sc, o, d, h);
+      const Material& m = sc.mat[h.prim];
+      if (k > 0) {  // Russian roulette (integrator.h:70-78)
+        const float q = fminf(fmaxf(thr.x, fmaxf(thr.y, thr.z)), 1.0f);
+        if (rng.next1d() >= q) break;
+        thr = thr / q;
+      }
+      if (m.le[0] > 0.f || m.le[1] > 0.f || m.le[2] > 0.f)
+        rad = rad + thr * v3(m.le[0], m.le[1], m.le[2]);
+      const V3 wo = -d;
+      V3 wi_l;
+      float pdf;
+      const V3 f = bxdf_sample(m, world_to_local(wo, s.dpdu, s.ns, s.dpdv),
+                               kFromCamera, rng, wi_l, pdf);
+      const V3 wi = local_to_world(wi_l, s.dpdu, s.ns, s.dpdv);
+      thr = thr * (f * cos_term(wo, wi, s.ns, s.ng, kFromCamera) / pdf);
+      o = s.pos;
+      d = wi;
+    }
+    if (has_nan(rad)) {
+      ++dropped;
+      continue;
+    }
+    ax += rad.x;
+    ay += rad.y;
+    az += rad.z;
+  }
+  const float k = (float)(a.spp > 0 ? a.spp : 1);
+  a.out[3 * p] = ax / k;
+  a.out[3 * p + 1] = ay / k;
+  a.out[3 * p + 2] = az / k;
+  if (dropped) atomicAdd(a.dropped, (unsigned long long)dropped);
+}
+
+void render_path_tracing(const SceneDev& sc, const PathArgs& a, cudaStream_t s) {
+  const int n = a.width * a.height;
+  path_trace_kernel<<<(n + 127) / 128, 128, 0, s>>>(sc, a);
+}
+
+}  // namespace pm

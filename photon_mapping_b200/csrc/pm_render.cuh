@@ -23,6 +23,16 @@ struct RenderArgs {
   int* err;            // bit 1: slots exhausted, bit 2: path stack full
 };
 
+struct PathArgs {
+  V3 cam_pos, cam_fwd, cam_right, cam_up;
+  float focal;
+  int width, height, spp, max_depth;
+  float* out;                    // height x width x 3, averaged
+  unsigned long long* dropped;   // NaN samples
+};
+
+void render_path_tracing(const SceneDev& sc, const PathArgs& a, cudaStream_t s);
+
 void render_rng_init(unsigned long long* st, int w, int h, cudaStream_t s);
 void render_camera(const SceneDev& sc, const RenderArgs& a, cudaStream_t s);
 void render_list_queries(const float4* slots, const float4* srec,

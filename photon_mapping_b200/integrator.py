@@ -98,3 +98,26 @@ class PhotonMapping:
         self.ctx.check(self.ctx.lib.pm_render(self.ctx.handle, C.addressof(cam), C.addressof(p),
                                               out.ctypes.data, C.addressof(st)), "pm_render")
         return out, st.as_dict()
+
+
+class PathTracing:
+    """PathTracing (integrator.h:51-106): the unidirectional reference
+    integrator, rendered on the device."""
+
+    def __init__(self, maxDepth: int = 100, ctx: Context | None = None):
+        self.ctx = ctx if ctx is not None else Context(0)
+        self.maxDepth = int(maxDepth)
+
+    def build(self, scene, seed: int = 1) -> None:  # integrator.h:58: nothing to do
+        pass
+
+    def render(self, camera, width: int, height: int, n_samples: int):
+        """tests/test_path_tracing.cpp:25-52 on the device: (image, NaN drops)."""
+        import numpy as np
+        out = np.empty((height, width, 3), np.float32)
+        dropped = C.c_int64(0)
+        cam = camera.as_struct()
+        self.ctx.check(self.ctx.lib.pm_render_path_tracing(
+            self.ctx.handle, C.addressof(cam), int(width), int(height), int(n_samples),
+            self.maxDepth, out.ctypes.data, C.byref(dropped)), "pm_render_path_tracing")
+        return out, int(dropped.value)

@@ -84,3 +84,44 @@ def test_multiple_gather_rays(ctx):
     img, st = pmi.render(cam, 16, 16, 2, n_gather=4)
     want, _ = oracle_render(mesh, pmi, cam, 16, 16, 2, n_gather=4)
     np.testing.assert_allclose(img, want, rtol=1e-4, atol=1e-6)
+
+
+def test_path_tracing_matches_oracle(ctx):
+    from photon_mapping_b200.integrator import PathTracing
+    for mesh in (S.cornell_box(4), S.caustics_scene(0, grid=16, subdiv=2)):
+        sc = S.Scene(ctx)
+        sc.setMesh(mesh)
+        sc.build()
+        cam = Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
+        pt = PathTracing(30, ctx=ctx)
+        img, dropped = pt.render(cam, 32, 24, 8)
+        want, wd = O.OracleScene(mesh).render_pt(cam.as_array(), 32, 24, 8, 30)
+        # same per-sample arithmetic and the same per-pixel sum order
+        np.testing.assert_array_equal(img, want)
+        assert dropped == wd
+
+
+def test_photon_mapping_converges_to_path_tracing(ctx):
+    """Image-level check (oracle part iii): the photon-map render and the
+    path-traced image of the same scene agree in the mean (photon mapping's
+    only bias is the kNN blur) and per pixel up to noise. Pixels seeing the
+    light (Le = 17) are left out of the per-pixel figure: their value is
+    the fraction of samples landing on the light, noisy at low spp."""
+    from photon_mapping_b200.integrator import PathTracing
+    mesh = S.cornell_box(0)
+    sc = S.Scene(ctx)
+    sc.setMesh(mesh)
+    sc.build()
+    cam = Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
+    ref, _ = PathTracing(100, ctx=ctx).render(cam, 64, 64, 8192)
+    mask = ref.max(axis=2) < 1.0
+    for fg, spp in ((1, 64), (0, 16)):
+        pmi = PhotonMapping(1000000, 100, 1.0, 100, fg, 100, ctx=ctx)
+        pmi.build(sc, seed=9)
+        img, _ = pmi.render(cam, 64, 64, spp, n_gather=16)
+        err = (img - ref)[mask]
+        bias = float(err.mean()) / float(ref[mask].mean())
+        rel = float(np.sqrt(np.mean(err ** 2))) / float(ref[mask].mean())
+        print(f"final gathering {fg}: mean bias {bias:+.4f}, relative RMSE {rel:.3f}")
+        assert abs(bias) < 0.02
+        assert rel < 0.3
