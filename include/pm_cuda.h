@@ -269,6 +269,24 @@ int pm_render(pm_ctx* ctx, const pm_camera* camera,
               const pm_render_params* params, float* out_rgb,
               pm_render_stats* stats);
 
+typedef struct pm_integrate_params {
+  int32_t k_global, k_caustics;  /* as in pm_render_params                */
+  int32_t final_gathering_depth;
+  int32_t max_depth;
+  int32_t n_gather;              /* 1 = the reference                      */
+  int32_t reserved;
+} pm_integrate_params;
+
+/* PhotonMapping::integrate (integrator.h:566-569), batched over n rays:
+ * rays holds 6 floats each {origin, direction}; rng_states[i] is the state
+ * of the caller's sampler for ray i (the reference's RNG: PCG32 with
+ * inc = 1, sampler.h:11-47) and comes back advanced by exactly the draws
+ * integrate makes. out_rgb[3i..3i+3) receives the radiance, unfiltered
+ * (the caller drops NaN or negative samples, examples/main.cpp:49-56). */
+int pm_integrate(pm_ctx* ctx, const float* rays, int64_t n,
+                 uint64_t* rng_states, const pm_integrate_params* params,
+                 float* out_rgb);
+
 /* PathTracing::integrate (integrator.h:51-106) inside the render loop of
  * tests/test_path_tracing.cpp:25-52: spp samples per pixel from a sampler
  * seeded j + width*i, NaN samples dropped but counted in the average.
@@ -278,6 +296,13 @@ int pm_render_path_tracing(pm_ctx* ctx, const pm_camera* camera,
                            int32_t width, int32_t height, int32_t spp,
                            int32_t max_depth, float* out_rgb,
                            int64_t* dropped_nan);
+
+/* PathTracing::integrate (integrator.h:60-105) for n given rays (6 floats
+ * each {origin, direction}) with their samplers' PCG32 states, advanced in
+ * place by the draws made; out_rgb receives each ray's radiance. */
+int pm_path_trace_rays(pm_ctx* ctx, const float* rays, int64_t n,
+                       uint64_t* rng_states, int32_t max_depth,
+                       float* out_rgb);
 
 #ifdef __cplusplus
 }

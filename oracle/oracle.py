@@ -56,6 +56,8 @@ def oracle_lib() -> C.CDLL:
             "orc_sincos": (None, [_vp, _i64, _vp, _vp]),
             "orc_render": (None, [_vp, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _vp, _vp, _vp]),
             "orc_render_pt": (None, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp]),
+            "orc_integrate": (None, [_vp, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp,
+                                     _vp]),
         })
     return _oracle
 
@@ -200,6 +202,20 @@ class OracleScene:
                             cph.shape[0], int(c_emitted), cam.ctypes.data, prm.ctypes.data,
                             out.ctypes.data, dropped.ctypes.data)
         return out, dropped
+
+    def integrate(self, global_photons, g_emitted, caustic_photons, c_emitted, rays6, states,
+                  k_global, k_caustics, fg_depth, max_depth, n_gather=1):
+        """PhotonMapping::integrate per ray; returns (radiance (n,3), advanced states)."""
+        g = _c(global_photons, np.float32).reshape(-1, 9)
+        cph = _c(caustic_photons, np.float32).reshape(-1, 9)
+        r = _c(rays6, np.float32).reshape(-1, 6)
+        st = np.array(states, dtype=np.uint64, copy=True)
+        prm = np.array([k_global, k_caustics, fg_depth, max_depth, n_gather], np.int32)
+        out = np.empty((r.shape[0], 3), np.float32)
+        self.lib.orc_integrate(self.h, g.ctypes.data, g.shape[0], int(g_emitted), cph.ctypes.data,
+                               cph.shape[0], int(c_emitted), r.ctypes.data, r.shape[0],
+                               st.ctypes.data, prm.ctypes.data, out.ctypes.data)
+        return out, st
 
     def render_pt(self, camera_arr, width, height, spp, max_depth):
         cam = _c(camera_arr, np.float32)

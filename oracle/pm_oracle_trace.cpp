@@ -665,3 +665,34 @@ void orc_render_pt(void* h, const float* cam, int W, int H, int spp, int max_dep
 }
 
 }  // extern "C"
+
+extern "C" {
+
+// PhotonMapping::integrate for n given rays (6 floats each) and sampler
+// states (advanced in place); iprm as in orc_render from k_global on:
+// {k_global, k_caustics, fg_depth, max_depth, n_gather}.
+void orc_integrate(void* h, const float* gph, int64_t gn, int64_t g_emitted,
+                   const float* cph, int64_t cn, int64_t c_emitted, const float* rays,
+                   int64_t n, uint64_t* states, const int32_t* iprm, float* out) {
+  RenderCtx c;
+  c.s = (const Scene*)h;
+  c.global = PhotonSet{gph, gn, g_emitted};
+  c.caustics = PhotonSet{cph, cn, c_emitted};
+  c.kg = iprm[0];
+  c.kc = iprm[1];
+  c.fg_depth = iprm[2];
+  c.max_depth = iprm[3];
+  c.n_gather = iprm[4];
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t i = 0; i < n; ++i) {
+    Rng rng{states[i]};
+    const float* r = rays + 6 * i;
+    const V rad = integrate(c, mk(r[0], r[1], r[2]), mk(r[3], r[4], r[5]), rng, 0);
+    out[3 * i] = rad.x;
+    out[3 * i + 1] = rad.y;
+    out[3 * i + 2] = rad.z;
+    states[i] = rng.state;
+  }
+}
+
+}  // extern "C"

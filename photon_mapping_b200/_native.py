@@ -63,6 +63,8 @@ _SIGNATURES = {
     "pm_scene_intersect": (C.c_int, [_vp, _vp, _i64, _vp]),
     "pm_photons_trace": (C.c_int, [_vp, C.c_int, C.c_uint64, _i64, C.c_int, _vp]),
     "pm_render": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
+    "pm_integrate": (C.c_int, [_vp, _vp, _i64, _vp, _vp, _vp]),
+    "pm_path_trace_rays": (C.c_int, [_vp, _vp, _i64, _vp, C.c_int32, _vp]),
     "pm_render_path_tracing": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                          _vp, _vp]),
     "pm_photonmap_radiance_noalloc": (C.c_int, [_vp, _i64, _vp, _i64, C.c_int, _i64, _vp, _vp]),

@@ -1,0 +1,7 @@
+// Drop-in for the reference's triangle.h: area lights and triangles are part of
+// the device scene (photon_mapping_b200/csrc/pm_scene.cuh); see scene.h.
+#ifndef PM_DROPIN_TRIANGLE_H
+#define PM_DROPIN_TRIANGLE_H
+#include "core.h"
+#include "sampler.h"
+#endif

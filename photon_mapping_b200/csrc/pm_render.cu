@@ -103,14 +103,24 @@ __global__ void __launch_bounds__(128)
     const int64_t base = srec * a.q_per_sample;
     int nq = 0;
     V3 direct = v3(0.f, 0.f, 0.f);
-    // examples/main.cpp:40-41 and Camera::sampleRay (camera.h:41-47)
-    const float u = (2.0f * ((float)j + rng.next1d()) - (float)a.width) / (float)a.height;
-    const float v = (2.0f * ((float)i + rng.next1d()) - (float)a.height) / (float)a.height;
-    const V3 pinhole = a.cam_pos + a.focal * a.cam_fwd;
-    const V3 sensor = a.cam_pos + u * a.cam_right + v * a.cam_up;
+    V3 ro, rd;
+    if (a.in_rays) {
+      // caller's ray (PhotonMapping::integrate): no camera draws
+      const float* r = a.in_rays + 6 * (int64_t)p;
+      ro = v3(r[0], r[1], r[2]);
+      rd = v3(r[3], r[4], r[5]);
+    } else {
+      // examples/main.cpp:40-41 and Camera::sampleRay (camera.h:41-47)
+      const float u = (2.0f * ((float)j + rng.next1d()) - (float)a.width) / (float)a.height;
+      const float v = (2.0f * ((float)i + rng.next1d()) - (float)a.height) / (float)a.height;
+      const V3 pinhole = a.cam_pos + a.focal * a.cam_fwd;
+      const V3 sensor = a.cam_pos + u * a.cam_right + v * a.cam_up;
+      ro = sensor;
+      rd = normalize(pinhole - sensor);
+    }
     Frame st[kPathStack];
     int sp = 0;
-    st[sp++] = Frame{sensor, normalize(pinhole - sensor), v3(1.f, 1.f, 1.f), 0};
+    st[sp++] = Frame{ro, rd, v3(1.f, 1.f, 1.f), 0};
     while (sp > 0) {
       const Frame f = st[--sp];
       if (f.depth >= a.max_depth) continue;
@@ -245,10 +255,11 @@ __global__ void resolve_kernel(const float4* __restrict__ slots,
                                const float* __restrict__ res, int npix,
                                int batch, int q_per_sample,
                                float4* __restrict__ accum,
-                               unsigned long long* __restrict__ dropped) {
+                               unsigned long long* __restrict__ dropped,
+                               float* __restrict__ raw) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npix) return;
-  float4 acc = accum[p];
+  float4 acc = raw ? make_float4(0.f, 0.f, 0.f, 0.f) : accum[p];
   unsigned nan_n = 0, neg_n = 0;
   for (int s = 0; s < batch; ++s) {
     const int64_t sidx = (int64_t)p * batch + s;
@@ -261,12 +272,19 @@ __global__ void resolve_kernel(const float4* __restrict__ slots,
       const V3 l = v3(res[3 * t], res[3 * t + 1], res[3 * t + 2]);
       rad = rad + v3(w.x, w.y, w.z) * l;
     }
+    if (raw) {  // integrate(): the radiance itself, no filtering
+      raw[3 * sidx] = rad.x;
+      raw[3 * sidx + 1] = rad.y;
+      raw[3 * sidx + 2] = rad.z;
+      continue;
+    }
     if (has_nan(rad)) { ++nan_n; continue; }
     if (rad.x < 0.f || rad.y < 0.f || rad.z < 0.f) { ++neg_n; continue; }
     acc.x += rad.x;
     acc.y += rad.y;
     acc.z += rad.z;
   }
+  if (raw) return;
   accum[p] = acc;
   if (nan_n) atomicAdd(dropped, (unsigned long long)nan_n);
   if (neg_n) atomicAdd(dropped + 1, (unsigned long long)neg_n);
@@ -311,9 +329,9 @@ void render_list_queries(const float4* slots, const float4* srec,
 
 void render_resolve(const float4* slots, const float4* srec, const float* res,
                     int npix, int batch, int q_per_sample, float4* accum,
-                    unsigned long long* dropped, cudaStream_t s) {
+                    unsigned long long* dropped, cudaStream_t s, float* raw) {
   resolve_kernel<<<(npix + 127) / 128, 128, 0, s>>>(
-      slots, srec, res, npix, batch, q_per_sample, accum, dropped);
+      slots, srec, res, npix, batch, q_per_sample, accum, dropped, raw);
 }
 
 void render_finish(const float4* accum, int npix, int spp, float* out,
@@ -333,15 +351,24 @@ __global__ void __launch_bounds__(128)
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= a.width * a.height) return;
   const int i = p / a.width, j = p % a.width;
-  Rng rng{(unsigned long long)(j + a.width * i)};
+  Rng rng{a.in_rays ? a.rng_states[p] : (unsigned long long)(j + a.width * i)};
   float ax = 0.f, ay = 0.f, az = 0.f;
   unsigned dropped = 0;
-  for (int sidx = 0; sidx < a.spp; ++sidx) {
-    const float u = (2.0f * ((float)j + rng.next1d()) - (float)a.width) / (float)a.height;
-    const float v = (2.0f * ((float)i + rng.next1d()) - (float)a.height) / (float)a.height;
-    const V3 pinhole = a.cam_pos + a.focal * a.cam_fwd;
-    const V3 sensor = a.cam_pos + u * a.cam_right + v * a.cam_up;
-    V3 o = sensor, d = normalize(pinhole - sensor);
+  const int spp = a.in_rays ? 1 : a.spp;
+  for (int sidx = 0; sidx < spp; ++sidx) {
+    V3 o, d;
+    if (a.in_rays) {  // caller's ray and sampler (PathTracing::integrate)
+      const float* r = a.in_rays + 6 * (int64_t)p;
+      o = v3(r[0], r[1], r[2]);
+      d = v3(r[3], r[4], r[5]);
+    } else {
+      const float u = (2.0f * ((float)j + rng.next1d()) - (float)a.width) / (float)a.height;
+      const float v = (2.0f * ((float)i + rng.next1d()) - (float)a.height) / (float)a.height;
+      const V3 pinhole = a.cam_pos + a.focal * a.cam_fwd;
+      const V3 sensor = a.cam_pos + u * a.cam_right + v * a.cam_up;
+      o = sensor;
+      d = normalize(pinhole - sensor);
+    }
     V3 rad = v3(0.f, 0.f, 0.f), thr = v3(1.f, 1.f, 1.f);
     for (int k = 0; k < a.max_depth; ++k) {
       Hit h;
@@ -365,6 +392,12 @@ __global__ void __launch_bounds__(128)
       o = s.pos;
       d = wi;
     }
+    if (a.in_rays) {  // the radiance itself, unfiltered
+      ax = rad.x;
+      ay = rad.y;
+      az = rad.z;
+      break;
+    }
     if (has_nan(rad)) {
       ++dropped;
       continue;
@@ -373,7 +406,8 @@ __global__ void __launch_bounds__(128)
     ay += rad.y;
     az += rad.z;
   }
-  const float k = (float)(a.spp > 0 ? a.spp : 1);
+  if (a.in_rays) a.rng_states[p] = rng.state;
+  const float k = (float)(a.in_rays ? 1 : (a.spp > 0 ? a.spp : 1));
   a.out[3 * p] = ax / k;
   a.out[3 * p + 1] = ay / k;
   a.out[3 * p + 2] = az / k;

@@ -20,6 +20,7 @@ struct RenderArgs {
   unsigned long long* rng_state;  // per pixel, kept across passes
   float4* slots;       // 4 float4 per query slot
   float4* sample_rec;  // per sample {direct radiance, query count bits}
+  const float* in_rays;  // null: camera rays; else 6 floats per pixel slot
   int* err;            // bit 1: slots exhausted, bit 2: path stack full
 };
 
@@ -29,6 +30,8 @@ struct PathArgs {
   int width, height, spp, max_depth;
   float* out;                    // height x width x 3, averaged
   unsigned long long* dropped;   // NaN samples
+  const float* in_rays;          // null: camera rays; else 6 floats per ray
+  unsigned long long* rng_states;  // with in_rays: per-ray sampler states
 };
 
 void render_path_tracing(const SceneDev& sc, const PathArgs& a, cudaStream_t s);
@@ -40,9 +43,11 @@ void render_list_queries(const float4* slots, const float4* srec,
                          const float* scene_lo, const float* scene_hi,
                          uint32_t* keys, uint32_t* vals, unsigned* count,
                          cudaStream_t s);
+// raw != null: write each sample's radiance there instead of accumulating
 void render_resolve(const float4* slots, const float4* srec, const float* res,
                     int npix, int batch, int q_per_sample, float4* accum,
-                    unsigned long long* dropped, cudaStream_t s);
+                    unsigned long long* dropped, cudaStream_t s,
+                    float* raw = nullptr);
 void render_finish(const float4* accum, int npix, int spp, float* out,
                    cudaStream_t s);
 

@@ -30,6 +30,12 @@ class RenderStats(C.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
 
 
+class IntegrateParams(C.Structure):
+    _fields_ = [("k_global", C.c_int32), ("k_caustics", C.c_int32),
+                ("final_gathering_depth", C.c_int32), ("max_depth", C.c_int32),
+                ("n_gather", C.c_int32), ("reserved", C.c_int32)]
+
+
 class TraceStats(C.Structure):
     _fields_ = [("emitted", C.c_int64), ("stored", C.c_int64),
                 ("nan_throughput", C.c_uint32), ("negative_throughput", C.c_uint32)]
@@ -81,6 +87,30 @@ class PhotonMapping:
             self.ctx.check(self.ctx.lib.pm_photonmap_build(self.ctx.handle, N.PM_MAP_CAUSTICS,
                                                            None, 0), "pm_photonmap_build")
         return self.stats
+
+    def integrate_batch(self, origins, directions, rng_states, n_gather: int = 1):
+        """PhotonMapping::integrate (integrator.h:566-569) for many rays, each
+        with its sampler's PCG32 state: returns (radiance (n, 3), states
+        advanced by the draws integrate made)."""
+        import numpy as np
+        o = np.asarray(origins, np.float32).reshape(-1, 3)
+        d = np.asarray(directions, np.float32).reshape(-1, 3)
+        rays = np.ascontiguousarray(np.concatenate([o, d], axis=1))
+        st = np.array(rng_states, dtype=np.uint64, copy=True).reshape(-1)
+        out = np.empty((rays.shape[0], 3), np.float32)
+        p = IntegrateParams(self.nEstimationGlobal, self.nEstimationGlobal,
+                            self.finalGatheringDepth, self.maxDepth, int(n_gather), 0)
+        self.ctx.check(self.ctx.lib.pm_integrate(self.ctx.handle, rays.ctypes.data, rays.shape[0],
+                                                 st.ctypes.data, C.addressof(p), out.ctypes.data),
+                       "pm_integrate")
+        return out, st
+
+    def integrate(self, ray, scene, sampler):
+        """integrator.h:566: radiance along one ray; `sampler` (a state
+        holder with a `state` attribute) advances like the reference's."""
+        out, st = self.integrate_batch([ray[0]], [ray[1]], [sampler.state])
+        sampler.state = int(st[0])
+        return out[0]
 
     def render(self, camera, width: int, height: int, n_samples: int, n_gather: int = 1,
                spp_batch: int = 0):

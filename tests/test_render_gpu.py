@@ -125,3 +125,24 @@ def test_photon_mapping_converges_to_path_tracing(ctx):
         print(f"final gathering {fg}: mean bias {bias:+.4f}, relative RMSE {rel:.3f}")
         assert abs(bias) < 0.02
         assert rel < 0.3
+
+
+@pytest.mark.parametrize("fg", [0, 1])
+def test_integrate_rays_match_oracle(ctx, fg):
+    """pm_integrate: arbitrary rays with their samplers' states; the radiance
+    matches the oracle and the states advance by the same draws."""
+    mesh = S.caustics_scene(0, grid=24, subdiv=2)
+    pmi = setup(ctx, mesh, 20000, 30, fg, 12, mult=2.0)
+    rng = np.random.default_rng(5)
+    n = 3000
+    o = rng.uniform(0.05, 0.95, (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3))
+    d = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    states = rng.integers(0, 2**63, n, dtype=np.uint64)
+    got, gst = pmi.integrate_batch(o, d, states)
+    want, wst = O.OracleScene(mesh).integrate(
+        pmi.global_map.photons(), pmi.nPhotonsGlobal, pmi.caustics_map.photons(),
+        pmi.nPhotonsCaustics, np.concatenate([o, d], axis=1), states, pmi.nEstimationGlobal,
+        pmi.nEstimationGlobal, pmi.finalGatheringDepth, pmi.maxDepth)
+    np.testing.assert_array_equal(gst, wst)
+    np.testing.assert_allclose(got, want, rtol=RTOL, atol=ATOL)
