@@ -201,12 +201,49 @@ RENDER_CONFIGS = {
     # 512^2, 1M photons, k=100, final gathering with 16 gather rays;
     # timed on 2 of its 100 spp (samples/s is per sample)
     "config2": dict(width=512, height=512, spp=2, photons=1_000_000, k=100, fg=1, n_gather=16),
+    # the same with the reference integrator's single gather ray per hit
+    # (integrator.h:292-309), the setting its CPU time is taken on
+    "config2_gather1": dict(width=512, height=512, spp=4, photons=1_000_000, k=100, fg=1,
+                            n_gather=1),
 }
+CPU_RENDER_BUDGET_S = 6.0   # per config, for the reference integrator's bounded sample
 
 
-def render_rates(ctx, sc, camera, dev) -> dict:
+def cpu_render_rate(mesh, pmi, c) -> dict | None:
+    """The reference's own PhotonMapping::integrate in the loop of
+    examples/main.cpp (oracle/_ref, compiled from the reference headers),
+    over the same photon maps, on a bounded band of rows in the middle of
+    the image. Returns the samples/s record."""
+    from oracle import oracle as O
+    from photon_mapping_b200 import scene as S
+    if c["n_gather"] != 1 or not O.ref_integrator_available():
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        path = Path(td) / "scene.obj"
+        S.write_obj(mesh, path)
+        ref = O.RefIntegrator(path)
+    ref.set_maps(pmi.global_map.photons(), pmi.caustics_map.photons(), c["photons"], c["k"],
+                 1.0, c["k"], c["fg"], MAX_DEPTH)
+    cam = S.CAMERA
+    w, h, spp = c["width"], c["height"], c["spp"]
+    args = (cam["position"], cam["forward"], cam["fov"], w, h, spp)
+    rows = 2
+    _, secs = ref.render(*args, h // 2 - 1, h // 2 + 1)
+    rows = int(min(max(rows * CPU_RENDER_BUDGET_S / max(secs, 1e-3), 2), h))
+    row0 = (h - rows) // 2
+    _, secs = ref.render(*args, row0, row0 + rows)
+    ref.close()
+    return {"value": rows * w * spp / secs, "unit": "samples/s", "cores": O.RefIntegrator.threads(),
+            "kind": "reference",
+            "sample": (f"rows {row0}-{row0 + rows - 1} of {w}x{h} at {spp} spp through the "
+                       f"reference's Scene + PhotonMapping (scene.h, integrator.h, g++ -O3 "
+                       f"-fopenmp) over the same photon maps, {secs:.1f} s")}
+
+
+def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
     """Camera samples per second of pm_render (host API, wall clock) for
-    the configs above, photon maps traced beforehand."""
+    the configs above, photon maps traced beforehand; beside each, the
+    reference integrator's CPU rate where its settings match."""
     import torch
     from photon_mapping_b200.integrator import PhotonMapping
     out = {}
@@ -222,6 +259,8 @@ def render_rates(ctx, sc, camera, dev) -> dict:
         out[name] = {"samples_per_s": n / dt, "seconds": dt, **c,
                      "queries_global": st["queries_global"], "passes": st["passes"],
                      "mean_radiance": float(img.mean())}
+        if cpu:
+            out[name]["cpu_reference"] = cpu_render_rate(mesh, pmi, c)
     return out
 
 
@@ -332,7 +371,8 @@ def run_ours(args) -> None:
     ctx.set_stats(False)
     per_q = {k2: v / max(st["queries"], 1) for k2, v in st.items() if k2 != "queries"}
 
-    render = {} if args.no_render else render_rates(ctx, sc, camera, dev)
+    render = {} if args.no_render else render_rates(
+        ctx, sc, mesh, camera, dev, cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -17,6 +17,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "liboracle.so"
 REF_PM_SO = HERE / "_ref" / "libpmref_photonmap.so"
+REF_INT_SO = HERE / "_ref" / "libpmref_integrator.so"
 
 _i64, _vp = C.c_int64, C.c_void_p
 
@@ -40,6 +41,7 @@ def _load(path: Path, sigs: dict) -> C.CDLL:
 
 _oracle = None
 _refpm = None
+_refint = None
 
 
 def oracle_lib() -> C.CDLL:
@@ -77,6 +79,95 @@ def ref_pm_lib() -> C.CDLL:
             "ref_pm_radiance": (None, [_vp, _vp, _i64, C.c_int, C.c_int, _vp]),
         })
     return _refpm
+
+
+def ref_integrator_available() -> bool:
+    return REF_INT_SO.exists()
+
+
+def ref_int_lib() -> C.CDLL:
+    global _refint
+    if _refint is None:
+        _refint = _load(REF_INT_SO, {
+            "ref_int_max_threads": (C.c_int, []),
+            "ref_int_new": (_vp, [C.c_char_p, C.c_char_p]),
+            "ref_int_free": (None, [_vp]),
+            "ref_int_build": (C.c_double, [_vp, C.c_int, C.c_int, C.c_float, C.c_int, C.c_int,
+                                           C.c_int]),
+            "ref_int_n_photons": (_i64, [_vp]),
+            "ref_int_set_maps": (None, [_vp, _vp, _i64, _vp, _i64, C.c_int, C.c_int, C.c_float,
+                                        C.c_int, C.c_int, C.c_int]),
+            "ref_int_render": (C.c_double, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, _vp]),
+            "ref_int_render_pt": (C.c_double, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                               C.c_int, C.c_int, _vp]),
+        })
+    return _refint
+
+
+class RefIntegrator:
+    """The reference's own Scene + PhotonMapping/PathTracing on the CPU
+    (include/scene.h, include/integrator.h compiled unchanged), over an
+    OBJ/MTL pair on disk. Rendering covers rows [row0, row1) and returns the
+    raw per-pixel mean (no gamma) and the seconds taken."""
+
+    def __init__(self, obj_path):
+        obj_path = Path(obj_path).resolve()
+        self.lib = ref_int_lib()
+        self.h = self.lib.ref_int_new(str(obj_path.parent).encode(), obj_path.name.encode())
+        if not self.h:
+            raise RuntimeError(f"reference Scene could not load {obj_path}")
+
+    @staticmethod
+    def threads() -> int:
+        return int(ref_int_lib().ref_int_max_threads())
+
+    def build(self, n_photons, n_est_global, caustics_multiplier, n_est_caustics, fg_depth,
+              max_depth) -> float:
+        """PhotonMapping(...) + build; returns seconds."""
+        return float(self.lib.ref_int_build(self.h, n_photons, n_est_global,
+                                            float(caustics_multiplier), n_est_caustics,
+                                            fg_depth, max_depth))
+
+    def set_maps(self, global_photons, caustic_photons, n_photons, n_est_global,
+                 caustics_multiplier, n_est_caustics, fg_depth, max_depth) -> None:
+        """A PhotonMapping whose two maps hold the given photons (no tracing)."""
+        g = _c(global_photons, np.float32).reshape(-1, 9)
+        cph = _c(caustic_photons, np.float32).reshape(-1, 9)
+        self.lib.ref_int_set_maps(self.h, g.ctypes.data, g.shape[0], cph.ctypes.data,
+                                  cph.shape[0], n_photons, n_est_global,
+                                  float(caustics_multiplier), n_est_caustics, fg_depth, max_depth)
+
+    def n_photons(self) -> int:
+        return int(self.lib.ref_int_n_photons(self.h))
+
+    def render(self, position, forward, fov, width, height, spp, row0=0, row1=None):
+        row1 = height if row1 is None else row1
+        cam = np.array([*position, *forward, fov], np.float32)
+        out = np.zeros((row1 - row0, width, 3), np.float32)
+        sec = self.lib.ref_int_render(self.h, cam.ctypes.data, width, height, spp, row0, row1,
+                                      out.ctypes.data)
+        return out, float(sec)
+
+    def render_pt(self, position, forward, fov, width, height, spp, max_depth, row0=0,
+                  row1=None):
+        row1 = height if row1 is None else row1
+        cam = np.array([*position, *forward, fov], np.float32)
+        out = np.zeros((row1 - row0, width, 3), np.float32)
+        sec = self.lib.ref_int_render_pt(self.h, cam.ctypes.data, width, height, spp, max_depth,
+                                         row0, row1, out.ctypes.data)
+        return out, float(sec)
+
+    def close(self):
+        if self.h:
+            self.lib.ref_int_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _c(a, dtype):
