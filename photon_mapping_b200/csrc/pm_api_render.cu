@@ -18,7 +18,7 @@ int render_buffers(pm_ctx* c, int npix, int64_t n_samples, int64_t n_slots) {
       (s = c->r_slots.ensure((size_t)n_slots * 64)) ||
       (s = c->r_srec.ensure((size_t)n_samples * 16)) ||
       (s = c->r_res.ensure((size_t)n_slots * 12)) ||
-      (s = c->r_sort.ensure((size_t)n_slots * 16 + 256 * (size_t)sort_tiles(n_slots) * 4 + 64)) ||
+      (s = c->r_sort.ensure((size_t)n_slots * 16 + sort_hist_words(n_slots) * 4 + 64)) ||
       (s = c->r_misc.ensure(64)) || (s = c->dev_err.ensure(64)) ||
       (s = c->q_out.ensure((size_t)npix * 12)))
     return set_err(c, s, "render buffers (%lld query slots)", (long long)n_slots);

@@ -47,7 +47,7 @@ constexpr size_t kNaBoxes = align256(noalloc_boxes(kNoAllocMaxPhotons) * 32);
 // map_build_scratch_bytes(n): keys/values a/b, tile histogram, box words
 constexpr size_t kNaSort =
     align256(4 * (size_t)kNoAllocMaxPhotons * 4 +
-             256 * (((size_t)kNoAllocMaxPhotons + kSortTile - 1) / kSortTile) * 4 + 64);
+             sort_hist_words(kNoAllocMaxPhotons) * 4 + 64);
 constexpr size_t kNaCounter = 256;
 constexpr size_t kNaBytes = kNaPos4 + kNaThr4 + kNaWi2 + kNaBoxes + kNaSort + kNaCounter;
 

@@ -41,7 +41,7 @@ int map_levels(int64_t n, int* nlevels, int* lvl_off, int* lvl_cnt) {
 size_t map_build_scratch_bytes(int64_t n) {
   const size_t nn = (size_t)(n > 0 ? n : 1);
   // keys a/b, values a/b, tile histogram, bbox words
-  return 4 * nn * sizeof(uint32_t) + 256 * (size_t)sort_tiles(nn) * 4 + 64;
+  return 4 * nn * sizeof(uint32_t) + sort_hist_words(nn) * 4 + 64;
 }
 
 __device__ __forceinline__ uint32_t ordered_bits(float f) {
@@ -199,7 +199,7 @@ void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
   uint32_t* va = kb + n;
   uint32_t* vb = va + n;
   uint32_t* hist = vb + n;
-  uint32_t* bb = hist + 256 * (size_t)sort_tiles(n);
+  uint32_t* bb = hist + sort_hist_words(n);
   cudaMemsetAsync(bb, 0xff, 3 * sizeof(uint32_t), st);
   cudaMemsetAsync(bb + 3, 0x00, 3 * sizeof(uint32_t), st);
   const int tb = 256;

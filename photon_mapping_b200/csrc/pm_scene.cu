@@ -220,7 +220,7 @@ __global__ void refit_kernel(const float4* __restrict__ mt, int n,
 size_t scene_build_scratch_bytes(int n) {
   const size_t nn = (size_t)(n > 1 ? n : 2);
   // keys a/b, vals a/b, hist, bbox, child (2n), parent (2n), flags (n)
-  return 4 * nn * 4 + 256 * (size_t)sort_tiles(nn) * 4 + 64 + 2 * nn * 4 +
+  return 4 * nn * 4 + sort_hist_words(nn) * 4 + 64 + 2 * nn * 4 +
          2 * nn * 4 + nn * 4;
 }
 
@@ -233,7 +233,7 @@ void scene_build_launch(const float* verts, const float* nrms, int n,
   uint32_t* va = kb + n;
   uint32_t* vb = va + n;
   uint32_t* hist = vb + n;
-  uint32_t* bb = hist + 256 * (size_t)sort_tiles(n);
+  uint32_t* bb = hist + sort_hist_words(n);
   int* child = (int*)(bb + 16);
   int* parent = child + 2 * (size_t)n;
   unsigned* flags = (unsigned*)(parent + 2 * (size_t)n);

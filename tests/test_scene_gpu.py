@@ -146,6 +146,21 @@ def test_trace_matches_oracle(ctx, small_caustics, map_id):
     assert want.shape[0] > (n_emit if map_id == 0 else 100)
 
 
+def test_trace_large_matches_oracle(ctx):
+    """More than 1M stored photons: the photon-order sort spans more than 256
+    tiles."""
+    mesh = S.cornell_box(2)
+    sc = S.Scene(ctx)
+    sc.setMesh(mesh)
+    sc.build()
+    st = trace_photons(ctx, 0, 11, 400000, 100)
+    got = PhotonMap(ctx, 0).photons()
+    want, _ = O.OracleScene(mesh).trace(0, 11, 0, 400000, 100)
+    assert want.shape[0] > 1_100_000
+    assert st["stored"] == want.shape[0]
+    np.testing.assert_array_equal(got, want)
+
+
 def test_photon_mapping_build_cornell(ctx):
     mesh = S.cornell_box(0)
     sc = S.Scene(ctx)
