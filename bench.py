@@ -53,6 +53,10 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-render", action="store_true", help="skip the render-rate measurements")
+    ap.add_argument("--convergence", type=int, nargs="*", default=None, metavar="CONFIG",
+                    help="instead of the benchmark: image error against the path tracer for "
+                         "these configs (default 1 2 3), beside the reference integrator's")
+    ap.add_argument("--pt-spp", type=int, default=4096)
     return ap.parse_args()
 
 
@@ -426,6 +430,53 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+# ------------------------------------------------------------------ convergence
+
+REF_BAND_BUDGET_S = 20.0
+
+
+def run_convergence(args) -> None:
+    """One JSON line per config: the device render's error against the
+    path-traced image (photon_mapping_b200.configs), and on a band of rows
+    the same error of the reference's own PhotonMapping (its own photon
+    tracing and camera pass, oracle/_ref, on the host cores) against the
+    same path-traced image. The reference integrator has one gather ray per
+    hit, so configs with more are reported without it."""
+    from oracle import oracle as O
+    from photon_mapping_b200 import Context
+    from photon_mapping_b200 import configs as CF
+    from photon_mapping_b200 import scene as S
+    ctx = Context(0)
+    for num in (args.convergence or sorted(CF.CONFIGS)):
+        rec, img, pt = CF.run_config(ctx, num, args.pt_spp, return_images=True)
+        c = CF.CONFIGS[num]
+        rec["reference"] = None
+        if c["n_gather"] == 1 and O.ref_integrator_available():
+            with tempfile.TemporaryDirectory() as td:
+                path = Path(td) / "scene.obj"
+                S.write_obj(CF.make_scene(c["scene"]), path)
+                ref = O.RefIntegrator(path)
+            t_build = ref.build(c["photons"], c["k"], c["caustics_multiplier"], c["k"], c["fg"],
+                                CF.MAX_DEPTH)
+            cam = S.CAMERA
+            w, h, spp = c["width"], c["height"], c["spp"]
+            a = (cam["position"], cam["forward"], cam["fov"], w, h, spp)
+            _, secs = ref.render(*a, h // 2 - 1, h // 2 + 1)
+            rows = int(min(max(2 * REF_BAND_BUDGET_S / max(secs, 1e-3), 2), h))
+            r0 = (h - rows) // 2
+            band, secs = ref.render(*a, r0, r0 + rows)
+            rec["reference"] = {
+                "rows": [r0, r0 + rows], "build_s": t_build, "render_s": secs,
+                "samples_per_s": rows * w * spp / secs, "cores": O.RefIntegrator.threads(),
+                "photons_stored_global": ref.n_photons(),
+                "error_vs_path_tracing": CF.image_error(band, pt[r0:r0 + rows]),
+                "ours_on_same_rows": CF.image_error(img[r0:r0 + rows], pt[r0:r0 + rows]),
+            }
+            ref.close()
+        print(json.dumps(rec), flush=True)
+    ctx.close()
+
+
 # -------------------------------------------------------------- reference arm
 
 def run_reference(args) -> None:
@@ -487,7 +538,9 @@ def run_reference(args) -> None:
 
 def main():
     args = parse_args()
-    if args.impl == "reference":
+    if args.convergence is not None:
+        run_convergence(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)
