@@ -304,6 +304,66 @@ int pm_path_trace_rays(pm_ctx* ctx, const float* rays, int64_t n,
                        uint64_t* rng_states, int32_t max_depth,
                        float* out_rgb);
 
+/* ------------------------------------------------- differentiable render
+ * The reference computes no gradients; these entry points extend its
+ * PhotonMapping::build + render loop (integrator.h:393-563, 290-377,
+ * examples/main.cpp:33-70) with the derivative of an image loss with
+ * respect to per-material Lambert albedos and the light emission.
+ *
+ * The parameters: n_params albedo parameters (RGB each), face f using
+ * parameter face_param[f] (-1: its material stays as uploaded), and one
+ * emission RGB that replaces Le of every emitting face. Parameter faces
+ * must be Lambertian. All parameters must be positive and finite.
+ *
+ * Photon paths are replayed from their per-photon seeds, never stored. The
+ * Russian-roulette decisions of the photon trace (integrator.h:441-449)
+ * depend on the throughput, hence on the albedos; the forward pass makes
+ * them with the "decision" parameters, so that a change of the albedos
+ * alone moves no path (frozen decisions) and the image is a smooth
+ * function of the parameters. With decision parameters equal to the
+ * parameters the forward pass is the plain render. */
+
+#define PM_DIFF_MAX_PARAMS 32
+
+/* Sets the albedo parameter of every face of the uploaded scene (n_faces
+ * entries in [-1, n_params)). Uploading a scene clears it. */
+int pm_diff_set_parameters(pm_ctx* ctx, const int32_t* face_param,
+                           int64_t n_faces, int32_t n_params);
+
+typedef struct pm_diff_params {
+  int32_t width, height, spp;
+  int32_t k;                     /* nEstimationGlobal, both maps
+                                    (integrator.h:139, :161)                 */
+  int32_t final_gathering_depth;
+  int32_t max_depth;
+  int32_t n_gather;              /* 1 = the reference                      */
+  int32_t reserved;
+  int64_t n_photons;             /* nPhotonsGlobal                         */
+  int64_t n_photons_caustics;    /* caustics map (final gathering only)    */
+  uint64_t seed;                 /* global map; the caustics map: seed + 1 */
+} pm_diff_params;
+
+/* Forward pass: writes albedo (n_params x 3) and emission (3) into the
+ * scene's materials, traces both photon maps with Russian-roulette
+ * decisions taken on decision_albedo / decision_emission (NULL: the
+ * parameters themselves), renders the image (as pm_render, all spp in one
+ * pass) into out_rgb (height x width x 3) and keeps what pm_diff_backward
+ * needs. stats may be NULL. */
+int pm_diff_forward(pm_ctx* ctx, const pm_camera* camera,
+                    const pm_diff_params* params, const float* albedo,
+                    const float* emission, const float* decision_albedo,
+                    const float* decision_emission, float* out_rgb,
+                    pm_render_stats* stats);
+
+/* Backward pass of the last pm_diff_forward on this context: given
+ * grad_rgb = d loss / d image (height x width x 3), writes d loss / d
+ * albedo (n_params x 3) and d loss / d emission (3). The hand-written
+ * adjoint runs the camera pass in reverse, scatters each estimate's adjoint
+ * onto its k nearest photons, and replays the photon paths from their
+ * seeds. */
+int pm_diff_backward(pm_ctx* ctx, const float* grad_rgb, float* grad_albedo,
+                     float* grad_emission);
+
 #ifdef __cplusplus
 }
 #endif

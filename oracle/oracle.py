@@ -60,6 +60,8 @@ def oracle_lib() -> C.CDLL:
             "orc_render_pt": (None, [_vp, _vp, C.c_int, C.c_int, C.c_int, C.c_int, _vp, _vp]),
             "orc_integrate": (None, [_vp, _vp, _i64, _i64, _vp, _i64, _i64, _vp, _i64, _vp, _vp,
                                      _vp]),
+            "orc_grad": (None, [_vp, _vp, C.c_int, C.c_uint64, _i64, _i64, _vp, _vp, _vp, _vp,
+                                _vp]),
         })
     return _oracle
 
@@ -307,6 +309,23 @@ class OracleScene:
                                cph.shape[0], int(c_emitted), r.ctypes.data, r.shape[0],
                                st.ctypes.data, prm.ctypes.data, out.ctypes.data)
         return out, st
+
+    def grad(self, face_param, n_params, seed, n_global, n_caustic, camera_arr, width, height,
+             spp, k, fg_depth, max_depth, n_gather, grad_img):
+        """FP64 forward-mode derivative of the traced-and-rendered image
+        (photon maps traced here: global with `seed`, caustics with seed + 1)
+        contracted with grad_img = d loss / d image. Returns (d loss / d
+        albedo (n_params, 3), d loss / d emission (3,), image)."""
+        pid = _c(face_param, np.int32)
+        cam = _c(camera_arr, np.float32)
+        prm = np.array([width, height, spp, k, fg_depth, max_depth, n_gather], np.int32)
+        gi = _c(grad_img, np.float32).reshape(height, width, 3)
+        out = np.zeros((n_params + 1) * 3, np.float64)
+        img = np.empty((height, width, 3), np.float32)
+        self.lib.orc_grad(self.h, pid.ctypes.data, int(n_params), C.c_uint64(seed), int(n_global),
+                          int(n_caustic), cam.ctypes.data, prm.ctypes.data, gi.ctypes.data,
+                          out.ctypes.data, img.ctypes.data)
+        return out[: 3 * n_params].reshape(n_params, 3), out[3 * n_params:], img
 
     def render_pt(self, camera_arr, width, height, spp, max_depth):
         cam = _c(camera_arr, np.float32)

@@ -696,3 +696,377 @@ void orc_integrate(void* h, const float* gph, int64_t gn, int64_t g_emitted,
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ gradient (forward mode)
+// FP64 CPU derivative of the image loss of the camera pass above with
+// respect to per-face albedo parameters and the light emission, by forward
+// differentiation: every throughput and radiance value carries, in double,
+// its derivative with respect to each parameter channel (albedos only
+// affect their own colour channel, so one derivative per parameter and
+// channel). Values themselves are computed in float exactly as above, so
+// the paths, the kNN sets and the dropped samples are the render's.
+// Russian-roulette decisions use the values (the derivative is that of the
+// estimator with these decisions held).
+namespace orc {
+
+constexpr int kGMax = 33;  // albedo parameters + emission
+
+struct DV {
+  V v;
+  double d[kGMax][3];
+};
+
+struct GradCtx {
+  RenderCtx rc;
+  const int* pid;  // per face
+  int np;          // albedo parameters; slot np is the emission
+  int nd;          // np + 1
+  const double* gtan;  // global photons' tangents, nd * 3 per photon
+  const double* ctan;  // caustics photons' tangents
+};
+
+static inline void dv_zero(DV& a, int nd) {
+  a.v = mk(0, 0, 0);
+  for (int x = 0; x < nd; ++x) a.d[x][0] = a.d[x][1] = a.d[x][2] = 0.0;
+}
+
+// a.d += s (per channel) * b.d
+static inline void dv_axpy(DV& a, const double s[3], const DV& b, int nd) {
+  for (int x = 0; x < nd; ++x)
+    for (int c = 0; c < 3; ++c) a.d[x][c] += s[c] * b.d[x][c];
+}
+
+static inline double comp(V v, int c) { return c == 0 ? v.x : (c == 1 ? v.y : v.z); }
+
+// Photon tracing with tangents (both rules), photons stored in (photon,
+// bounce) order with nd * 3 doubles each.
+static void trace_tan(const Scene& s, const int* pid, int nd, int map, uint64_t seed,
+                      int64_t n_emit, int max_depth, std::vector<float>& ph,
+                      std::vector<double>& tan) {
+  const int np = nd - 1;
+  std::vector<double> t((size_t)nd * 3);
+  for (int64_t i = 0; i < n_emit; ++i) {
+    Rng rng{splitmix64(seed ^ splitmix64((uint64_t)i))};
+    float pc, pp, pd;
+    const int lf = sample_light(s, rng, pc);
+    const Surf ls = sample_point(s, lf, rng, pp);
+    float u0, u1;
+    rng.next2(u0, u1);
+    V dir = to_world(cos_hemisphere(u0, u1, pd), ls.dpdu, ls.ns, ls.dpdv);
+    const Mat& lm = s.mat[lf];
+    V thr = muls(divs(mk(lm.le[0], lm.le[1], lm.le[2]), pc * pp * pd), std::fabs(dot(dir, ls.ns)));
+    std::fill(t.begin(), t.end(), 0.0);
+    const double dle = 1.0 / ((double)pc * pp * pd) * std::fabs((double)dot(dir, ls.ns));
+    for (int c = 0; c < 3; ++c) t[3 * np + c] = dle;
+    V org = ls.pos;
+    bool prev_specular = false;
+    for (int k = 0; k < max_depth; ++k) {
+      if (std::isnan(thr.x) || std::isnan(thr.y) || std::isnan(thr.z)) break;
+      if (thr.x < 0 || thr.y < 0 || thr.z < 0) break;
+      Hit hit;
+      if (!intersect(s, org, dir, RAY_EPS, 3.40282347e+38f, hit)) break;
+      const Surf sf = surface(s, org, dir, hit);
+      const Mat& m = s.mat[hit.prim];
+      const bool diffuse = m.type == 0;
+      bool store = false, stop = false;
+      if (map == 0) {
+        store = diffuse;
+      } else {
+        if (!prev_specular && diffuse) break;
+        if (prev_specular && diffuse) store = stop = true;
+        prev_specular = !diffuse;
+      }
+      if (store) {
+        const V wi = neg(dir);
+        const float rec[9] = {thr.x, thr.y, thr.z, sf.pos.x, sf.pos.y, sf.pos.z, wi.x, wi.y, wi.z};
+        ph.insert(ph.end(), rec, rec + 9);
+        tan.insert(tan.end(), t.begin(), t.end());
+      }
+      if (stop) break;
+      double qinv = 1.0;
+      if (k > 0) {
+        const float q = std::min(std::max(thr.x, std::max(thr.y, thr.z)), 1.0f);
+        if (rng.next() >= q) break;
+        thr = divs(thr, q);
+        qinv = 1.0 / (double)q;
+      }
+      const V wo = neg(dir);
+      V wil;
+      float pdf;
+      const V wol = to_local(wo, sf.dpdu, sf.ns, sf.dpdv);
+      const V f = sample_bxdf(m, wol, 0, rng, wil, pdf);
+      const V wi = to_world(wil, sf.dpdu, sf.ns, sf.dpdv);
+      const float ct = cos_term(wo, wi, sf.ns, sf.ng, 0);
+      // thr' = (thr / q) f ct / pdf: the tangent t (not yet divided by q)
+      // becomes t f ct / (pdf q) + (thr / q) (d f / d albedo) ct / pdf
+      const int p = pid[hit.prim];
+      const bool valid = diffuse && !(wol.y < 0 || wil.y < 0);
+      for (int x = 0; x < nd; ++x)
+        for (int c = 0; c < 3; ++c) t[3 * x + c] *= comp(f, c) * (double)ct / (double)pdf * qinv;
+      if (p >= 0 && valid)
+        for (int c = 0; c < 3; ++c)
+          t[3 * p + c] += comp(thr, c) * (1.0 / (double)PI) * (double)ct / (double)pdf;
+      thr = mul(thr, divs(muls(f, ct), pdf));
+      org = sf.pos;
+      dir = wi;
+    }
+  }
+}
+
+// Lambert f at a surface of material m with parameter p: value (float, as
+// lambert_eval) and d f_c / d albedo_c = 1/pi when the directions pass.
+static DV estimate_d(const GradCtx& g, const PhotonSet& pm, const double* tan, int k,
+                     const Surf& sf, V wo, const Mat& m, int p) {
+  DV r;
+  dv_zero(r, g.nd);
+  if (pm.n == 0) return r;
+  std::vector<std::pair<float, int>> c;
+  c.reserve((size_t)pm.n);
+  for (int64_t i = 0; i < pm.n; ++i) {
+    const float* ph = pm.p + 9 * i;
+    float d2 = 0.f;
+    d2 += (sf.pos.x - ph[3]) * (sf.pos.x - ph[3]);
+    d2 += (sf.pos.y - ph[4]) * (sf.pos.y - ph[4]);
+    d2 += (sf.pos.z - ph[5]) * (sf.pos.z - ph[5]);
+    if (!std::isnan(d2)) c.push_back({d2, (int)i});
+  }
+  const size_t kk = std::min<size_t>((size_t)k, c.size());
+  std::partial_sort(c.begin(), c.begin() + kk, c.end());
+  float maxd2 = 0.f;
+  for (size_t q = 0; q < kk; ++q) maxd2 = std::max(maxd2, c[q].first);
+  V lo = mk(0, 0, 0);
+  const V wo_l = to_local(wo, sf.dpdu, sf.ns, sf.dpdv);
+  for (size_t q = kk; q-- > 0;) {
+    const int idx = c[q].second;
+    const float* ph = pm.p + 9 * idx;
+    const V wi_l = to_local(mk(ph[6], ph[7], ph[8]), sf.dpdu, sf.ns, sf.dpdv);
+    const V f = lambert_eval(m, wo_l, wi_l);
+    lo = add(lo, mul(f, mk(ph[0], ph[1], ph[2])));
+    const bool valid = !(wo_l.y < 0 || wi_l.y < 0);
+    if (!valid) continue;
+    const double* t = tan + (size_t)idx * 3 * g.nd;
+    for (int x = 0; x < g.nd; ++x)
+      for (int ch = 0; ch < 3; ++ch) r.d[x][ch] += comp(f, ch) * t[3 * x + ch];
+    if (p >= 0)
+      for (int ch = 0; ch < 3; ++ch) r.d[p][ch] += (1.0 / (double)PI) * (double)ph[ch];
+  }
+  if (kk > 0) {
+    const float den = (float)pm.emitted * PI * maxd2;
+    lo = divs(lo, den);
+    for (int x = 0; x < g.nd; ++x)
+      for (int ch = 0; ch < 3; ++ch) r.d[x][ch] /= (double)den;
+  }
+  r.v = lo;
+  return r;
+}
+
+static DV direct_d(const GradCtx& g, const Surf& sf, V wo, const Mat& m, int p, Rng& rng) {
+  const Scene& s = *g.rc.s;
+  DV r;
+  dv_zero(r, g.nd);
+  float pc, pp;
+  const int lf = sample_light(s, rng, pc);
+  const Surf ls = sample_point(s, lf, rng, pp);
+  const V wi = normalize(sub(ls.pos, sf.pos));
+  const float rr = length(sub(ls.pos, sf.pos));
+  const float pd = pp * rr * rr / std::fabs(dot(neg(wi), ls.ns));
+  Hit h;
+  if (intersect(s, sf.pos, wi, RAY_EPS, rr - RAY_EPS, h)) return r;
+  const Mat& lm = s.mat[lf];
+  const V wol = to_local(wo, sf.dpdu, sf.ns, sf.dpdv), wil = to_local(wi, sf.dpdu, sf.ns, sf.dpdv);
+  const V f = lambert_eval(m, wol, wil);
+  const float cs = std::fabs(dot(wi, sf.ns));
+  const V le = mk(lm.le[0], lm.le[1], lm.le[2]);
+  r.v = divs(mul(muls(f, cs), le), pc * pd);
+  const double k = (double)cs / ((double)pc * (double)pd);
+  for (int c = 0; c < 3; ++c) r.d[g.np][c] = comp(f, c) * k;  // d / d Le_c
+  if (p >= 0 && !(wol.y < 0 || wil.y < 0))
+    for (int c = 0; c < 3; ++c) r.d[p][c] += (1.0 / (double)PI) * k * comp(le, c);
+  return r;
+}
+
+static DV indirect_d(const GradCtx& g, V wo, const Surf& sf, const Mat& m, int p, Rng& rng,
+                     int depth) {
+  DV r;
+  dv_zero(r, g.nd);
+  const RenderCtx& c = g.rc;
+  if (depth >= c.max_depth) return r;
+  V wil;
+  float pdf;
+  const V wol = to_local(wo, sf.dpdu, sf.ns, sf.dpdv);
+  const V f = sample_bxdf(m, wol, 1, rng, wil, pdf);
+  const V dir = to_world(wil, sf.dpdu, sf.ns, sf.dpdv);
+  const float cs = std::fabs(dot(sf.ns, dir));
+  Hit h;
+  if (!intersect(*c.s, sf.pos, dir, RAY_EPS, 3.40282347e+38f, h)) return r;
+  const Surf s2 = surface(*c.s, sf.pos, dir, h);
+  const Mat& m2 = c.s->mat[h.prim];
+  DV x;
+  if (m2.type == 0)
+    x = estimate_d(g, c.global, g.gtan, c.kg, s2, neg(dir), m2, g.pid[h.prim]);
+  else
+    x = indirect_d(g, neg(dir), s2, m2, g.pid[h.prim], rng, depth + 1);
+  r.v = divs(mul(muls(f, cs), x.v), pdf);
+  double s3[3];
+  for (int ch = 0; ch < 3; ++ch) s3[ch] = comp(f, ch) * (double)cs / (double)pdf;
+  dv_axpy(r, s3, x, g.nd);
+  if (p >= 0 && m.type == 0 && !(wol.y < 0 || wil.y < 0))
+    for (int ch = 0; ch < 3; ++ch)
+      r.d[p][ch] += (1.0 / (double)PI) * (double)cs / (double)pdf * comp(x.v, ch);
+  return r;
+}
+
+static DV integrate_d(const GradCtx& g, V o, V d, Rng& rng, int depth) {
+  DV r;
+  dv_zero(r, g.nd);
+  const RenderCtx& c = g.rc;
+  if (depth >= c.max_depth) return r;
+  Hit h;
+  if (!intersect(*c.s, o, d, RAY_EPS, 3.40282347e+38f, h)) return r;
+  const Surf sf = surface(*c.s, o, d, h);
+  const Mat& m = c.s->mat[h.prim];
+  const int p = g.pid[h.prim];
+  if (m.le[0] > 0 || m.le[1] > 0 || m.le[2] > 0) {
+    r.v = mk(m.le[0], m.le[1], m.le[2]);
+    for (int ch = 0; ch < 3; ++ch) r.d[g.np][ch] = 1.0;
+    return r;
+  }
+  const V wo = neg(d);
+  if (m.type == 0) {
+    if (depth >= c.fg_depth) return estimate_d(g, c.global, g.gtan, c.kg, sf, wo, m, p);
+    const DV ld = direct_d(g, sf, wo, m, p, rng);
+    const DV lc = estimate_d(g, c.caustics, g.ctan, c.kc, sf, wo, m, p);
+    DV li;
+    dv_zero(li, g.nd);
+    const float ig = 1.0f / (float)c.n_gather;
+    const double one[3] = {1.0, 1.0, 1.0}, igd[3] = {ig, ig, ig};
+    for (int gi = 0; gi < c.n_gather; ++gi) {
+      const DV x = indirect_d(g, wo, sf, m, p, rng, 0);
+      li.v = add(li.v, muls(x.v, ig));
+      dv_axpy(li, igd, x, g.nd);
+    }
+    r.v = add(add(ld.v, lc.v), li.v);
+    dv_axpy(r, one, ld, g.nd);
+    dv_axpy(r, one, lc, g.nd);
+    dv_axpy(r, one, li, g.nd);
+    return r;
+  }
+  const V wo_l = to_local(wo, sf.dpdu, sf.ns, sf.dpdv);
+  if (depth >= 3) {
+    V wil;
+    float pdf;
+    const V f = sample_bxdf(m, wo_l, 1, rng, wil, pdf);
+    const V wi = to_world(wil, sf.dpdu, sf.ns, sf.dpdv);
+    const V thr = divs(muls(f, cos_term(wo, wi, sf.ns, sf.ng, 1)), pdf);
+    const DV x = integrate_d(g, sf.pos, wi, rng, depth + 1);
+    r.v = mul(thr, x.v);
+    const double s3[3] = {thr.x, thr.y, thr.z};
+    dv_axpy(r, s3, x, g.nd);
+    return r;
+  }
+  V dirs[2], fs[2];
+  int nb = 0;
+  if (m.type == 1) {
+    dirs[0] = reflect(wo_l, mk(0, 1, 0));
+    fs[0] = divs(rho(m), std::fabs(dirs[0].y));
+    nb = 1;
+  } else {
+    float iorO, iorI;
+    V n;
+    if (wo_l.y > 0) { iorO = 1.0f; iorI = m.ior; n = mk(0, 1, 0); }
+    else { iorO = m.ior; iorI = 1.0f; n = mk(0, -1, 0); }
+    const float fr = fresnel(dot(wo_l, n), iorO, iorI);
+    dirs[0] = reflect(wo_l, n);
+    fs[0] = divs(muls(rho(m), fr), std::fabs(dirs[0].y));
+    nb = 1;
+    V tr;
+    if (refract(wo_l, n, iorO, iorI, tr)) {
+      const float sc = (iorO * iorO) / (iorI * iorI);
+      dirs[1] = tr;
+      fs[1] = divs(muls(rho(m), (1.0f - fr) * sc), std::fabs(tr.y));
+      nb = 2;
+    } else {
+      fs[0] = divs(rho(m), std::fabs(dirs[0].y));
+    }
+  }
+  for (int b = 0; b < nb; ++b) {
+    const V wi = to_world(dirs[b], sf.dpdu, sf.ns, sf.dpdv);
+    const V thr = muls(fs[b], std::fabs(dot(wi, sf.ns)));
+    const DV x = integrate_d(g, sf.pos, wi, rng, depth + 1);
+    r.v = add(r.v, mul(thr, x.v));
+    const double s3[3] = {thr.x, thr.y, thr.z};
+    dv_axpy(r, s3, x, g.nd);
+  }
+  return r;
+}
+
+}  // namespace orc
+
+extern "C" {
+
+// Traces both maps (global: seed; caustics, with final gathering: seed + 1)
+// and renders like orc_render, and returns out_grad[(np + 1) * 3]: d loss /
+// d albedo parameter (np x 3) then d loss / d emission (3), for
+// d loss / d image = grad_img (height x width x 3). pid: parameter of each
+// face (-1: none). out_img receives the image.
+// iprm: {width, height, spp, k, fg_depth, max_depth, n_gather}.
+void orc_grad(void* h, const int32_t* pid, int np, uint64_t seed, int64_t n_global,
+              int64_t n_caustic, const float* cam, const int32_t* iprm,
+              const float* grad_img, double* out_grad, float* out_img) {
+  const Scene& s = *(const Scene*)h;
+  const int nd = np + 1;
+  const int W = iprm[0], H = iprm[1], spp = iprm[2];
+  std::vector<float> gph, cph;
+  std::vector<double> gtan, ctan;
+  trace_tan(s, pid, nd, 0, seed, n_global, iprm[5], gph, gtan);
+  if (iprm[4] > 0) trace_tan(s, pid, nd, 1, seed + 1, n_caustic, iprm[5], cph, ctan);
+  GradCtx g;
+  g.rc.s = &s;
+  g.rc.global = PhotonSet{gph.data(), (int64_t)(gph.size() / 9), n_global};
+  g.rc.caustics = PhotonSet{cph.data(), (int64_t)(cph.size() / 9), n_caustic};
+  g.rc.kg = g.rc.kc = iprm[3];
+  g.rc.fg_depth = iprm[4];
+  g.rc.max_depth = iprm[5];
+  g.rc.n_gather = iprm[6];
+  g.pid = pid;
+  g.np = np;
+  g.nd = nd;
+  g.gtan = gtan.data();
+  g.ctan = ctan.data();
+  const V pos = mk(cam[0], cam[1], cam[2]), fwd = mk(cam[3], cam[4], cam[5]);
+  const V right = mk(cam[6], cam[7], cam[8]), up = mk(cam[9], cam[10], cam[11]);
+  const float focal = cam[12];
+  std::vector<double> acc((size_t)nd * 3, 0.0);
+#pragma omp parallel
+  {
+    std::vector<double> mine((size_t)nd * 3, 0.0);
+#pragma omp for schedule(dynamic, 1)
+    for (int p = 0; p < W * H; ++p) {
+      const int i = p / W, j = p % W;
+      Rng rng{(uint64_t)(j + W * i)};
+      V a = mk(0, 0, 0);
+      for (int k = 0; k < spp; ++k) {
+        const float u = (2.0f * (j + rng.next()) - W) / H;
+        const float v = (2.0f * (i + rng.next()) - H) / H;
+        const V pinhole = add(pos, muls(fwd, focal));
+        const V sensor = add(add(pos, muls(right, u)), muls(up, v));
+        const DV rad = integrate_d(g, sensor, normalize(sub(pinhole, sensor)), rng, 0);
+        const V rv = rad.v;
+        if (std::isnan(rv.x) || std::isnan(rv.y) || std::isnan(rv.z)) continue;
+        if (rv.x < 0 || rv.y < 0 || rv.z < 0) continue;
+        a = add(a, rv);
+        for (int x = 0; x < nd; ++x)
+          for (int c = 0; c < 3; ++c)
+            mine[3 * x + c] += (double)grad_img[3 * p + c] / (double)spp * rad.d[x][c];
+      }
+      out_img[3 * p] = a.x / (float)spp;
+      out_img[3 * p + 1] = a.y / (float)spp;
+      out_img[3 * p + 2] = a.z / (float)spp;
+    }
+#pragma omp critical
+    for (size_t t = 0; t < acc.size(); ++t) acc[t] += mine[t];
+  }
+  for (size_t t = 0; t < acc.size(); ++t) out_grad[t] = acc[t];
+}
+
+}  // extern "C"

@@ -68,6 +68,9 @@ _SIGNATURES = {
     "pm_render_path_tracing": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                          _vp, _vp]),
     "pm_photonmap_radiance_noalloc": (C.c_int, [_vp, _i64, _vp, _i64, C.c_int, _i64, _vp, _vp]),
+    "pm_diff_set_parameters": (C.c_int, [_vp, _vp, _i64, C.c_int32]),
+    "pm_diff_forward": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "pm_diff_backward": (C.c_int, [_vp, _vp, _vp, _vp]),
 }
 
 

@@ -78,6 +78,7 @@ int build_map(pm_ctx* c, DevMap& dm, const float* d_aos, int64_t n,
                    (long long)n);
   int st_ok;
   dm.built = false;
+  c->diff.ready = false;
   dm.n = n;
   int total = map_levels(n, &dm.nlevels, dm.lvl_off, dm.lvl_cnt);
   if (n == 0) {

@@ -6,6 +6,7 @@
 #include <mutex>
 #include <string>
 
+#include "../../include/pm_cuda.h"
 #include "pm_photonmap.cuh"
 #include "pm_scene.cuh"
 
@@ -38,6 +39,7 @@ struct DevMap {
 };
 
 struct DevScene {
+  uint64_t generation = 0;  // bumped by every upload
   int64_t n_faces = 0;
   int n_lights = 0;
   bool has_specular = false;
@@ -50,6 +52,32 @@ struct DevScene {
     verts_in.release(); nrms_in.release();
     built = false;
     n_faces = 0;
+  }
+};
+
+// State of the differentiable render between pm_diff_forward and
+// pm_diff_backward.
+struct DiffState {
+  uint64_t scene_generation = ~0ull;  // scene the parameters were set for
+  int n_params = 0;
+  DevBuf face_pid, base_mat, dec_mat, theta, grad;
+  DevBuf first[2];      // first stored photon of each emitted photon, per map
+  DevBuf photon_adj[2]; // d loss / d throughput per stored photon, per map
+  DevBuf slot_pid, nee, nee_count, slot_adj;
+  // the last forward pass
+  bool ready = false;
+  int width = 0, height = 0, spp = 0, q_per_sample = 0, k = 0, max_depth = 0;
+  int fg_depth = 0;
+  uint64_t seed = 0;
+  int64_t emitted[2] = {0, 0};
+  float theta_host[3 * 33] = {};  // albedos then emission of the last forward
+  void release() {
+    face_pid.release(); base_mat.release(); dec_mat.release(); theta.release();
+    grad.release(); first[0].release(); first[1].release();
+    photon_adj[0].release(); photon_adj[1].release();
+    slot_pid.release(); nee.release(); nee_count.release(); slot_adj.release();
+    ready = false;
+    scene_generation = ~0ull;
   }
 };
 
@@ -77,6 +105,7 @@ struct pm_ctx {
   pm::DevBuf counter;      // kCounterRing work counters
   unsigned counter_next = 0;
   pm::DevBuf stats;        // pm_knn_stats counters (device)
+  pm::DiffState diff;      // differentiable render
   bool stats_on = false;
   unsigned long long* stats_ptr() {
     return stats_on ? (unsigned long long*)stats.ptr : nullptr;
@@ -101,6 +130,7 @@ struct pm_ctx {
     trace_misc.release();
     r_rng.release(); r_accum.release(); r_slots.release(); r_srec.release();
     r_res.release(); r_sort.release(); r_misc.release();
+    diff.release();
   }
   pm::SceneDev scene_view() const {
     pm::SceneDev v;
@@ -124,4 +154,10 @@ int cuda_status(pm_ctx* c, cudaError_t e, const char* where);
 MapDev map_view(const DevMap& dm);
 int build_map(pm_ctx* c, DevMap& dm, const float* d_aos, int64_t n,
               cudaStream_t st);
+int take_device_error(pm_ctx* c, const char* where);
+// Traces `map` (the body of pm_photons_trace; the caller holds the lock).
+// dmat: decision materials (frozen decisions) or null; first: receives the
+// first stored photon of each emitted photon, or null.
+int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
+              const Material* dmat, DevBuf* first, pm_trace_stats* stats);
 }  // namespace pm

@@ -1,6 +1,7 @@
 // C ABI of the camera pass: pm_render, pm_integrate, pm_render_path_tracing.
 #include "../../include/pm_cuda.h"
 #include "pm_api_internal.cuh"
+#include "pm_api_render.cuh"
 #include "pm_render.cuh"
 #include "pm_sort.cuh"
 
@@ -8,11 +9,12 @@ using namespace pm;
 
 static_assert(sizeof(pm_camera) == 13 * 4, "camera layout");
 
-namespace {
+namespace pm {
 
 // Buffers of the camera pipeline: npix pixel (or ray) slots, n_samples
 // samples per pass, n_slots query slots per pass.
 int render_buffers(pm_ctx* c, int npix, int64_t n_samples, int64_t n_slots) {
+  c->diff.ready = false;  // the camera buffers are about to be reused
   int s;
   if ((s = c->r_rng.ensure((size_t)npix * 8)) || (s = c->r_accum.ensure((size_t)npix * 16)) ||
       (s = c->r_slots.ensure((size_t)n_slots * 64)) ||
@@ -27,8 +29,11 @@ int render_buffers(pm_ctx* c, int npix, int64_t n_samples, int64_t n_slots) {
 
 // Answers the photon-map queries a camera pass wrote: per map, list the
 // slots holding one, sort them by Morton code, run the radiance kernel.
+// With slot_adj, runs the adjoint instead: the neighbours of each slot
+// receive slot_adj times d estimate / d throughput in photon_adj[map].
 int answer_queries(pm_ctx* c, const RenderArgs& a, int64_t ns, int64_t n_slots,
-                   bool need_caustics, int kg, int kc, int64_t* q_tot) {
+                   bool need_caustics, int kg, int kc, int64_t* q_tot,
+                   const float* slot_adj, float4* const* photon_adj) {
   cudaStream_t st = c->stream;
   uint32_t* ka = (uint32_t*)c->r_sort.ptr;
   uint32_t* kb = ka + n_slots;
@@ -53,9 +58,11 @@ int answer_queries(pm_ctx* c, const RenderArgs& a, int64_t ns, int64_t n_slots,
     KnnOut o{};
     o.rgb = (float*)c->r_res.ptr;
     o.stats = c->stats_ptr();
-    e = knn_launch(map_view(c->maps[map]), a.slots, nq, map == 0 ? kg : kc, kModeRadiance,
-                   (float)c->map_emitted[map], o, c->next_counter(), c->num_sms, st,
-                   in_b ? vb : va, 4);
+    o.adj_in = slot_adj;
+    o.photon_adj = slot_adj ? photon_adj[map] : nullptr;
+    e = knn_launch(map_view(c->maps[map]), a.slots, nq, map == 0 ? kg : kc,
+                   slot_adj ? kModeAdjoint : kModeRadiance, (float)c->map_emitted[map], o,
+                   c->next_counter(), c->num_sms, st, in_b ? vb : va, 4);
     if (e != cudaSuccess) return cuda_status(c, e, "render estimates");
   }
   return PM_OK;
@@ -88,7 +95,7 @@ int slots_per_sample(const pm_ctx* c, bool need_caustics, int n_gather) {
   return (c->scene.has_specular ? 8 : 1) * per_leaf;
 }
 
-}  // namespace
+}  // namespace pm
 
 extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
                          const pm_render_params* prm, float* out_rgb,
@@ -147,7 +154,7 @@ extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
     const int64_t ns = (int64_t)npix * b;
     render_camera(sv, a, st);
     if ((s = answer_queries(c, a, ns, n_slots, need_caustics, p.k_global, p.k_caustics,
-                            q_tot)) != PM_OK)
+                            q_tot, nullptr, nullptr)) != PM_OK)
       return s;
     render_resolve(a.slots, a.sample_rec, (const float*)c->r_res.ptr, npix, b, q_per_sample,
                    (float4*)c->r_accum.ptr, dropped, st);
@@ -219,7 +226,7 @@ extern "C" int pm_integrate(pm_ctx* c, const float* rays, int64_t n,
   render_camera(c->scene_view(), a, st);
   int64_t q_tot[2] = {0, 0};
   if ((s = answer_queries(c, a, npix, n_slots, need_caustics, p.k_global, p.k_caustics,
-                          q_tot)) != PM_OK)
+                          q_tot, nullptr, nullptr)) != PM_OK)
     return s;
   render_resolve(a.slots, a.sample_rec, (const float*)c->r_res.ptr, npix, 1, q_per_sample,
                  (float4*)c->r_accum.ptr, (unsigned long long*)c->r_misc.ptr, st,

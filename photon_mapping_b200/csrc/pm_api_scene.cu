@@ -29,7 +29,7 @@ static int ensure_err(pm_ctx* c) {
 
 // Reads and clears the device error word; a set bit is a kernel-reported
 // failure (bit 0: BVH traversal stack overflow).
-static int take_device_error(pm_ctx* c, const char* where) {
+int take_device_error(pm_ctx* c, const char* where) {
   int e = 0;
   cudaError_t ce = cudaMemcpyAsync(&e, c->dev_err.ptr, sizeof(int),
                                    cudaMemcpyDeviceToHost, c->stream);
@@ -39,6 +39,85 @@ static int take_device_error(pm_ctx* c, const char* where) {
     cudaMemsetAsync(c->dev_err.ptr, 0, sizeof(int), c->stream);
     return set_err(c, PM_ERR_DEVICE_STATUS, "%s: device error bits 0x%x",
                    where, e);
+  }
+  return PM_OK;
+}
+
+}  // namespace pm
+
+namespace pm {
+
+int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
+              const Material* dmat, DevBuf* first, pm_trace_stats* stats) {
+  c->diff.ready = false;  // the photon maps are about to change
+  if (!c->scene.built) return set_err(c, PM_ERR_NOT_BUILT, "scene not built");
+  if (n_emit > 0 && c->scene.n_lights == 0)
+    return set_err(c, PM_ERR_INVALID_ARGUMENT, "scene has no area light");
+  cudaStream_t st = c->stream;
+  cudaError_t e;
+  int s;
+  if ((s = c->trace_misc.ensure(64)) != PM_OK)
+    return set_err(c, s, "trace counters");
+  unsigned long long* counter = (unsigned long long*)c->trace_misc.ptr;
+  unsigned* status = (unsigned*)((char*)c->trace_misc.ptr + 16);
+  // capacity guess: 4 stored photons per emitted one; retried when short
+  unsigned long long cap = (unsigned long long)(n_emit > 0 ? n_emit : 1) * 4;
+  unsigned long long stored = 0;
+  unsigned hstatus[2] = {0, 0};
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    if ((s = c->trace_raw.ensure(cap * 36)) || (s = c->trace_keys.ensure(cap * 8)))
+      return set_err(c, s, "trace buffers (%llu photons)", cap);
+    if ((e = cudaMemsetAsync(c->trace_misc.ptr, 0, 64, st)) != cudaSuccess)
+      return cuda_status(c, e, "trace counters");
+    TraceArgs a{};
+    a.seed = seed;
+    a.n_emit = (int)n_emit;
+    a.max_depth = max_depth;
+    a.caustic = map == PM_MAP_CAUSTICS;
+    a.out = (float*)c->trace_raw.ptr;
+    a.keys = (unsigned long long*)c->trace_keys.ptr;
+    a.counter = counter;
+    a.cap = cap;
+    a.status = status;
+    a.dmat = dmat;
+    trace_launch(c->scene_view(), a, st);
+    if ((e = cudaGetLastError()) != cudaSuccess)
+      return cuda_status(c, e, "trace launch");
+    if ((e = cudaMemcpyAsync(&stored, counter, 8, cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaMemcpyAsync(hstatus, status, 8, cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaStreamSynchronize(st)))
+      return cuda_status(c, e, "trace");
+    if ((s = take_device_error(c, "trace")) != PM_OK) return s;
+    if (stored <= cap) break;
+    cap = stored;  // the trace is deterministic: rerun with room for all
+  }
+  if (stored > (unsigned long long)0x7fffffff)
+    return set_err(c, PM_ERR_INVALID_ARGUMENT, "%llu photons stored", stored);
+  DevMap& dm = c->maps[map];
+  const int n = (int)stored;
+  if (first && (s = first->ensure((size_t)(n_emit > 0 ? n_emit : 1) * 4)) != PM_OK)
+    return set_err(c, s, "photon offsets");
+  if (n > 0) {
+    if ((s = dm.aos.ensure((size_t)n * 36)) ||
+        (s = c->scratch.ensure(order_scratch_bytes(n))))
+      return set_err(c, s, "photon order buffers");
+    // photon index < 2^31, bounce < 2^8: 39-bit keys
+    order_photons_launch((unsigned long long*)c->trace_keys.ptr,
+                         (const float*)c->trace_raw.ptr, n, 40,
+                         (float*)dm.aos.ptr, c->scratch.ptr, st,
+                         first ? (uint32_t*)first->ptr : nullptr);
+    if ((e = cudaGetLastError()) != cudaSuccess)
+      return cuda_status(c, e, "photon order");
+  }
+  if ((s = build_map(c, dm, (const float*)dm.aos.ptr, n, st)) != PM_OK) return s;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
+    return cuda_status(c, e, "photon map build");
+  c->map_emitted[map] = n_emit;
+  if (stats) {
+    stats->emitted = n_emit;
+    stats->stored = (int64_t)stored;
+    stats->nan_throughput = hstatus[0];
+    stats->negative_throughput = hstatus[1];
   }
   return PM_OK;
 }
@@ -61,6 +140,7 @@ int pm_scene_upload(pm_ctx* c, const float* vertices, const float* normals,
   cudaSetDevice(c->device);
   DevScene& sc = c->scene;
   sc.built = false;
+  ++sc.generation;
   int s;
   if ((s = ensure_err(c)) != PM_OK) return set_err(c, s, "error word");
   // area lights in face order (scene.h:41-51, :245-252)
@@ -158,72 +238,7 @@ int pm_photons_trace(pm_ctx* c, int map, uint64_t seed, int64_t n_emit,
                    (long long)n_emit, max_depth);
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
-  if (!c->scene.built) return set_err(c, PM_ERR_NOT_BUILT, "scene not built");
-  if (n_emit > 0 && c->scene.n_lights == 0)
-    return set_err(c, PM_ERR_INVALID_ARGUMENT, "scene has no area light");
-  cudaStream_t st = c->stream;
-  cudaError_t e;
-  int s;
-  if ((s = c->trace_misc.ensure(64)) != PM_OK)
-    return set_err(c, s, "trace counters");
-  unsigned long long* counter = (unsigned long long*)c->trace_misc.ptr;
-  unsigned* status = (unsigned*)((char*)c->trace_misc.ptr + 16);
-  // capacity guess: 4 stored photons per emitted one; retried when short
-  unsigned long long cap = (unsigned long long)(n_emit > 0 ? n_emit : 1) * 4;
-  unsigned long long stored = 0;
-  unsigned hstatus[2] = {0, 0};
-  for (int attempt = 0; attempt < 2; ++attempt) {
-    if ((s = c->trace_raw.ensure(cap * 36)) || (s = c->trace_keys.ensure(cap * 8)))
-      return set_err(c, s, "trace buffers (%llu photons)", cap);
-    if ((e = cudaMemsetAsync(c->trace_misc.ptr, 0, 64, st)) != cudaSuccess)
-      return cuda_status(c, e, "trace counters");
-    TraceArgs a;
-    a.seed = seed;
-    a.n_emit = (int)n_emit;
-    a.max_depth = max_depth;
-    a.caustic = map == PM_MAP_CAUSTICS;
-    a.out = (float*)c->trace_raw.ptr;
-    a.keys = (unsigned long long*)c->trace_keys.ptr;
-    a.counter = counter;
-    a.cap = cap;
-    a.status = status;
-    trace_launch(c->scene_view(), a, st);
-    if ((e = cudaGetLastError()) != cudaSuccess)
-      return cuda_status(c, e, "trace launch");
-    if ((e = cudaMemcpyAsync(&stored, counter, 8, cudaMemcpyDeviceToHost, st)) ||
-        (e = cudaMemcpyAsync(hstatus, status, 8, cudaMemcpyDeviceToHost, st)) ||
-        (e = cudaStreamSynchronize(st)))
-      return cuda_status(c, e, "trace");
-    if ((s = take_device_error(c, "trace")) != PM_OK) return s;
-    if (stored <= cap) break;
-    cap = stored;  // the trace is deterministic: rerun with room for all
-  }
-  if (stored > (unsigned long long)0x7fffffff)
-    return set_err(c, PM_ERR_INVALID_ARGUMENT, "%llu photons stored", stored);
-  DevMap& dm = c->maps[map];
-  const int n = (int)stored;
-  if (n > 0) {
-    if ((s = dm.aos.ensure((size_t)n * 36)) ||
-        (s = c->scratch.ensure(order_scratch_bytes(n))))
-      return set_err(c, s, "photon order buffers");
-    // photon index < 2^31, bounce < 2^8: 39-bit keys
-    order_photons_launch((unsigned long long*)c->trace_keys.ptr,
-                         (const float*)c->trace_raw.ptr, n, 40,
-                         (float*)dm.aos.ptr, c->scratch.ptr, st);
-    if ((e = cudaGetLastError()) != cudaSuccess)
-      return cuda_status(c, e, "photon order");
-  }
-  if ((s = build_map(c, dm, (const float*)dm.aos.ptr, n, st)) != PM_OK) return s;
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
-    return cuda_status(c, e, "photon map build");
-  c->map_emitted[map] = n_emit;
-  if (stats) {
-    stats->emitted = n_emit;
-    stats->stored = (int64_t)stored;
-    stats->nan_throughput = hstatus[0];
-    stats->negative_throughput = hstatus[1];
-  }
-  return PM_OK;
+  return trace_map(c, map, seed, n_emit, max_depth, nullptr, nullptr, stats);
 }
 
 }  // extern "C"

@@ -749,8 +749,8 @@ __global__ void __launch_bounds__(256, 4)
       q.k = k;
       q.cnt = 0;
       q.tau = kInf;
-      const int64_t rec = (MODE == kModeRadiance && order) ? (int64_t)__ldg(order + qi) : qi;
-      if (MODE == kModeRadiance) {
+      const int64_t rec = (MODE != kModeKnn && order) ? (int64_t)__ldg(order + qi) : qi;
+      if (MODE != kModeKnn) {
         // radiance record r0 = {pos, rho.r}; wo, ns and the other albedo
         // channels are read after the search
         const float4 r0 =
@@ -826,7 +826,33 @@ __global__ void __launch_bounds__(256, 4)
       const int kept = all ? cnt : k;
       const float maxd2 = kept > 0 ? __uint_as_float(kth_key) : 0.f;
 
-      if (MODE == kModeRadiance) {
+      if (MODE == kModeAdjoint) {
+        // d estimate / d throughput_i = f(wo, wi_i) / (n_emitted pi maxd2)
+        // for the kept photons (integrator.h:141-150)
+        const float4* q4 =
+            reinterpret_cast<const float4*>(queries) + stride4 * rec;
+        const float4 r0 = __ldg(q4);
+        const float4 r1 = __ldg(q4 + 1);
+        const float4 r2 = __ldg(q4 + 2);
+        const float ax = out.adj_in[3 * rec], ay = out.adj_in[3 * rec + 1],
+                    az = out.adj_in[3 * rec + 2];
+        const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
+        if (kept > 0 && (ax != 0.f || ay != 0.f || az != 0.f)) {
+          const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
+          const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
+          const float cr = __fdiv_rn(__fmul_rn(ax, __fdiv_rn(r0.w, kPI)), den);
+          const float cg = __fdiv_rn(__fmul_rn(ay, __fdiv_rn(r1.w, kPI)), den);
+          const float cb = __fdiv_rn(__fmul_rn(az, __fdiv_rn(r2.w, kPI)), den);
+          for (int i = lane; i < nk; i += 32) {
+            const uint32_t id = s.id[i];
+            const float4 t = __ldg(m.thr4 + id);
+            const float2 w = __ldg(m.wi2 + id);
+            const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
+            if (!(cos_o < 0.f) && !(cos_i < 0.f))
+              atomicAdd(out.photon_adj + orig_index(m.pos4, id), make_float4(cr, cg, cb, 0.f));
+          }
+        }
+      } else if (MODE == kModeRadiance) {
         // r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b}
         const float4* q4 =
             reinterpret_cast<const float4*>(queries) + stride4 * rec;
@@ -951,6 +977,12 @@ cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                        unsigned long long* counter, int num_sms,
                        cudaStream_t st, const uint32_t* order, int stride4) {
   if (nq <= 0) return cudaSuccess;
+  if (mode == kModeAdjoint) {
+    return k <= 224 ? launch_one<512, kModeAdjoint>(m, queries, nq, k, n_emitted, out, counter,
+                                                   num_sms, st, order, stride4)
+                    : launch_one<2048, kModeAdjoint>(m, queries, nq, k, n_emitted, out, counter,
+                                                    num_sms, st, order, stride4);
+  }
   if (k <= 224) {
     return mode == kModeRadiance
                ? launch_one<512, kModeRadiance>(m, queries, nq, k, n_emitted,

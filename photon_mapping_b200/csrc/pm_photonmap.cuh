@@ -46,7 +46,7 @@ void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
                       const int* lvl_cnt, int nlevels, void* scratch,
                       cudaStream_t st);
 
-enum KnnMode { kModeRadiance = 0, kModeKnn = 1 };
+enum KnnMode { kModeRadiance = 0, kModeKnn = 1, kModeAdjoint = 2 };
 
 struct KnnOut {
   float* rgb;          // radiance mode: 3 floats per record
@@ -54,6 +54,9 @@ struct KnnOut {
   int32_t* count;      // knn mode
   float* maxd2;        // knn mode
   unsigned long long* stats;  // 6 counters (pm_knn_stats) or null
+  const float* adj_in;  // adjoint mode: d loss / d estimate, 3 floats per record
+  float4* photon_adj;   // adjoint mode: d loss / d throughput per photon
+                        // (index order, .xyz), accumulated atomically
 };
 
 // Launches the warp-per-query k-nearest-neighbour kernel.
@@ -61,6 +64,9 @@ struct KnnOut {
 //                  pm_radiance_query at queries + stride4 * r float4s, and
 //                  writes rgb[3r .. 3r+3)
 //   knn mode:      queries = 3 floats per query (order and stride unused)
+//   adjoint mode:  the records of radiance mode; the neighbours of record r
+//                  receive adj_in[3r .. 3r+3) times d estimate / d
+//                  throughput in photon_adj
 // `counter` is one device word of scratch (reset by this call).
 cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                        int k, int mode, float n_emitted, KnnOut out,

@@ -30,13 +30,16 @@ struct Frame {
   int depth;
 };
 
+template <bool D>
 __device__ __forceinline__ void emit_query(const RenderArgs& a, int64_t base,
                                            int& nq, int map, const Surf& s,
-                                           V3 wo, V3 rho, V3 w) {
+                                           V3 wo, V3 rho, V3 w, int pid_w,
+                                           int pid_q) {
   if (nq >= a.q_per_sample) {
     atomicOr(a.err, 2);
     return;
   }
+  if (D) a.slot_pid[base + nq] = make_int2(pid_w, pid_q);
   float4* r = a.slots + 4 * (base + nq);
   r[0] = make_float4(s.pos.x, s.pos.y, s.pos.z, rho.x);
   r[1] = make_float4(wo.x, wo.y, wo.z, rho.y);
@@ -66,10 +69,12 @@ __device__ V3 direct_light(const SceneDev& sc, const Surf& s, V3 wo,
 
 // PhotonMapping::computeIndirectIlluminationRecursive (integrator.h:
 // 215-262) for one gather ray: a diffuse hit becomes a global-map query
-// with the accumulated weight, a specular hit continues the path.
+// with the accumulated weight, a specular hit continues the path. pid_w is
+// the albedo parameter of the surface the gather starts from.
+template <bool D>
 __device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
                        const Material* m, V3 w, Rng& rng, int64_t base,
-                       int& nq) {
+                       int& nq, int pid_w) {
   for (int depth = 0; depth < a.max_depth; ++depth) {
     V3 wi_l;
     float pdf;
@@ -83,7 +88,8 @@ __device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
     const Material* m2 = sc.mat + h.prim;
     w = w * (f * c / pdf);
     if (m2->type == kLambert) {
-      emit_query(a, base, nq, kQueryGlobal, s2, -dir, mat_rho(*m2), w);
+      emit_query<D>(a, base, nq, kQueryGlobal, s2, -dir, mat_rho(*m2), w, pid_w,
+                    D ? a.face_pid[h.prim] : -1);
       return;
     }
     s = s2;
@@ -92,6 +98,7 @@ __device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
   }
 }
 
+template <bool D>
 __global__ void __launch_bounds__(128)
     camera_kernel(SceneDev sc, RenderArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -101,7 +108,7 @@ __global__ void __launch_bounds__(128)
   for (int sidx = 0; sidx < a.batch; ++sidx) {
     const int64_t srec = (int64_t)p * a.batch + sidx;
     const int64_t base = srec * a.q_per_sample;
-    int nq = 0;
+    int nq = 0, nn = 0;
     V3 direct = v3(0.f, 0.f, 0.f);
     V3 ro, rd;
     if (a.in_rays) {
@@ -134,14 +141,18 @@ __global__ void __launch_bounds__(128)
         continue;
       }
       if (m.type == kLambert) {
+        const int pid = D ? a.face_pid[h.prim] : -1;
         if (f.depth >= a.fg_depth) {
-          emit_query(a, base, nq, kQueryGlobal, s, wo, mat_rho(m), f.w);
+          emit_query<D>(a, base, nq, kQueryGlobal, s, wo, mat_rho(m), f.w, -1, pid);
         } else {
-          direct = direct + f.w * direct_light(sc, s, wo, m, rng);
-          emit_query(a, base, nq, kQueryCaustics, s, wo, mat_rho(m), f.w);
+          const V3 ld = f.w * direct_light(sc, s, wo, m, rng);
+          direct = direct + ld;
+          if (D && nn < a.q_per_sample)
+            a.nee[base + nn++] = make_float4(ld.x, ld.y, ld.z, __int_as_float(pid));
+          emit_query<D>(a, base, nq, kQueryCaustics, s, wo, mat_rho(m), f.w, -1, pid);
           const V3 wg = f.w * a.inv_gather;
           for (int g = 0; g < a.n_gather; ++g)
-            gather(a, sc, s, wo, &m, wg, rng, base, nq);
+            gather<D>(a, sc, s, wo, &m, wg, rng, base, nq, pid);
         }
         continue;
       }
@@ -190,6 +201,7 @@ __global__ void __launch_bounds__(128)
       }
     }
     a.sample_rec[srec] = make_float4(direct.x, direct.y, direct.z, __int_as_float(nq));
+    if (D) a.nee_count[srec] = nn;
   }
   a.rng_state[p] = rng.state;
 }
@@ -308,7 +320,10 @@ void render_rng_init(unsigned long long* st, int w, int h, cudaStream_t s) {
 
 void render_camera(const SceneDev& sc, const RenderArgs& a, cudaStream_t s) {
   const int n = a.width * a.height;
-  camera_kernel<<<(n + 127) / 128, 128, 0, s>>>(sc, a);
+  if (a.slot_pid)
+    camera_kernel<true><<<(n + 127) / 128, 128, 0, s>>>(sc, a);
+  else
+    camera_kernel<false><<<(n + 127) / 128, 128, 0, s>>>(sc, a);
 }
 
 void render_list_queries(const float4* slots, const float4* srec,

@@ -22,6 +22,14 @@ struct RenderArgs {
   float4* sample_rec;  // per sample {direct radiance, query count bits}
   const float* in_rays;  // null: camera rays; else 6 floats per pixel slot
   int* err;            // bit 1: slots exhausted, bit 2: path stack full
+  // Differentiable render (null otherwise): what the adjoint pass needs to
+  // split each sample's radiance by albedo parameter.
+  const int* face_pid;  // albedo parameter of each face, -1 for none
+  int2* slot_pid;       // per slot {parameter whose BSDF scaled the weight,
+                        //           parameter of the query surface}
+  float4* nee;          // per sample, q_per_sample records {next-event
+                        // radiance, parameter of the surface (int bits)}
+  int* nee_count;       // per sample
 };
 
 struct PathArgs {

@@ -44,10 +44,20 @@ __device__ __forceinline__ void store_photon(const TraceArgs& a, int photon,
   a.keys[slot] = ((unsigned long long)photon << 8) | (unsigned)bounce;
 }
 
-__global__ void __launch_bounds__(128)
-    trace_kernel(SceneDev sc, TraceArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= a.n_emit) return;
+enum { kTracePlain = 0, kTraceFrozen = 1, kTraceReplay = 2 };
+
+// Shared accumulators of the replay: per block, the parameter sums and, per
+// thread, how many times each parameter has scaled the throughput so far.
+struct ReplaySmem {
+  float g[kMaxDiffParams * 3];
+  unsigned char cnt[kMaxDiffParams][128];
+};
+
+// One emitted photon of PhotonMapping::build (integrator.h:406-469 global,
+// :483-558 caustics).
+template <int MODE>
+__device__ __forceinline__ void trace_one(const SceneDev& sc, const TraceArgs& a, int i,
+                                          ReplaySmem* rs) {
   Rng rng{photon_stream_state(a.seed, (unsigned long long)i)};
 
   // sampleRayFromLight (integrator.h:265-288)
@@ -61,16 +71,25 @@ __global__ void __launch_bounds__(128)
   const Material& lm = sc.mat[lf];
   V3 thr = v3(lm.le[0], lm.le[1], lm.le[2]) /
            (pdf_choose * pdf_pos * pdf_dir) * fabsf(dot(dir, ls.ns));
+  // decision throughput: the same arithmetic over the decision materials
+  V3 td = thr;
+  if (MODE != kTracePlain) {
+    const Material& dm = a.dmat[lf];
+    td = v3(dm.le[0], dm.le[1], dm.le[2]) /
+         (pdf_choose * pdf_pos * pdf_dir) * fabsf(dot(dir, ls.ns));
+  }
   V3 org = ls.pos;
+  int nst = 0;  // replay: photons this path has stored so far
 
   bool prev_specular = false;
   for (int k = 0; k < a.max_depth; ++k) {
-    if (has_nan(thr)) {
-      atomicAdd(a.status + 0, 1u);
+    const V3 dec = MODE != kTracePlain ? td : thr;
+    if (has_nan(dec)) {
+      if (MODE != kTraceReplay) atomicAdd(a.status + 0, 1u);
       break;
     }
-    if (thr.x < 0.f || thr.y < 0.f || thr.z < 0.f) {
-      atomicAdd(a.status + 1, 1u);
+    if (dec.x < 0.f || dec.y < 0.f || dec.z < 0.f) {
+      if (MODE != kTraceReplay) atomicAdd(a.status + 1, 1u);
       break;
     }
     Hit h;
@@ -79,23 +98,46 @@ __global__ void __launch_bounds__(128)
     const Surf s = surface_at(sc, org, dir, h);
     const Material& m = sc.mat[h.prim];
     const bool diffuse = m.type == kLambert;
+    bool store = false, stop = false;
     if (!a.caustic) {
-      if (diffuse) store_photon(a, i, k, thr, s.pos, -dir);
+      store = diffuse;
     } else {
       // integrator.h:510-523
       if (!prev_specular && diffuse) break;
-      if (prev_specular && diffuse) {
-        store_photon(a, i, k, thr, s.pos, -dir);
-        break;
-      }
+      if (prev_specular && diffuse) store = stop = true;
       prev_specular = !diffuse;
     }
+    if (store) {
+      if (MODE == kTraceReplay) {
+        // the replay stores where the trace stored; cap = photons stored
+        const unsigned long long si = (unsigned long long)a.first[i] + (unsigned)nst;
+        if (si >= a.cap) {
+          atomicOr(sc.err, 8);
+          break;
+        }
+        const float4 g = a.adj[si];
+        const V3 w = v3(g.x, g.y, g.z) * thr;
+        for (int j = 0; j < a.n_params; ++j) {
+          const unsigned c = rs->cnt[j][threadIdx.x];
+          if (c) {
+            atomicAdd(&rs->g[3 * j + 0], (float)c * w.x);
+            atomicAdd(&rs->g[3 * j + 1], (float)c * w.y);
+            atomicAdd(&rs->g[3 * j + 2], (float)c * w.z);
+          }
+        }
+      } else {
+        store_photon(a, i, k, thr, s.pos, -dir);
+      }
+      ++nst;
+    }
+    if (stop) break;
     // Russian roulette (integrator.h:441-449)
     if (k > 0) {
       const float q =
-          fminf(fmaxf(thr.x, fmaxf(thr.y, thr.z)), 1.0f);
+          fminf(fmaxf(dec.x, fmaxf(dec.y, dec.z)), 1.0f);
       if (rng.next1d() >= q) break;
       thr = thr / q;
+      if (MODE != kTracePlain) td = td / q;
     }
     // Primitive::sampleBxDF FROM_LIGHT (primitive.h:46-62)
     const V3 wo = -dir;
@@ -104,10 +146,40 @@ __global__ void __launch_bounds__(128)
     float pdf;
     const V3 f = bxdf_sample(m, wo_l, kFromLight, rng, wi_l, pdf);
     const V3 wi = local_to_world(wi_l, s.dpdu, s.ns, s.dpdv);
-    thr = thr * (f * cos_term(wo, wi, s.ns, s.ng, kFromLight) / pdf);
+    const float ct = cos_term(wo, wi, s.ns, s.ng, kFromLight);
+    thr = thr * (f * ct / pdf);
+    if (MODE != kTracePlain) {
+      // albedo parameters sit on Lambert faces only; the direction drawn
+      // does not depend on the albedo
+      const V3 fd = diffuse ? lambert_eval(a.dmat[h.prim], wo_l, wi_l) : f;
+      td = td * (fd * ct / pdf);
+    }
+    if (MODE == kTraceReplay) {
+      const int pid = a.face_pid[h.prim];
+      if (pid >= 0) ++rs->cnt[pid][threadIdx.x];
+    }
     org = s.pos;
     dir = wi;
   }
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128)
+    trace_kernel(SceneDev sc, TraceArgs a) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (MODE == kTraceReplay) {
+    __shared__ ReplaySmem rs;
+    for (int t = threadIdx.x; t < 3 * a.n_params; t += blockDim.x) rs.g[t] = 0.f;
+    for (int j = 0; j < a.n_params; ++j) rs.cnt[j][threadIdx.x] = 0;
+    __syncthreads();
+    if (i < a.n_emit) trace_one<MODE>(sc, a, i, &rs);
+    __syncthreads();
+    for (int t = threadIdx.x; t < 3 * a.n_params; t += blockDim.x)
+      if (rs.g[t] != 0.f) atomicAdd(a.grad + t, (double)rs.g[t]);
+    return;
+  }
+  if (i >= a.n_emit) return;
+  trace_one<MODE>(sc, a, i, nullptr);
 }
 
 __global__ void gather_photons_kernel(const float* __restrict__ raw,
@@ -121,6 +193,15 @@ __global__ void gather_photons_kernel(const float* __restrict__ raw,
   for (int j = 0; j < 9; ++j) o[j] = r[j];
 }
 
+// first[p] = sorted index of the first stored photon of emitted photon p.
+__global__ void first_of_photon_kernel(const unsigned long long* __restrict__ keys,
+                                       int n, uint32_t* __restrict__ first) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= n) return;
+  const unsigned long long p = keys[s] >> 8;
+  if (s == 0 || (keys[s - 1] >> 8) != p) first[p] = (uint32_t)s;
+}
+
 __global__ void iota_kernel(uint32_t* v, int n) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) v[i] = (uint32_t)i;
@@ -128,8 +209,14 @@ __global__ void iota_kernel(uint32_t* v, int n) {
 
 void trace_launch(const SceneDev& sc, const TraceArgs& a, cudaStream_t st) {
   if (a.n_emit <= 0) return;
-  const int tb = 128;
-  trace_kernel<<<(a.n_emit + tb - 1) / tb, tb, 0, st>>>(sc, a);
+  const int tb = 128;  // ReplaySmem holds 128 threads' counters
+  const int gb = (a.n_emit + tb - 1) / tb;
+  if (a.adj)
+    trace_kernel<kTraceReplay><<<gb, tb, 0, st>>>(sc, a);
+  else if (a.dmat)
+    trace_kernel<kTraceFrozen><<<gb, tb, 0, st>>>(sc, a);
+  else
+    trace_kernel<kTracePlain><<<gb, tb, 0, st>>>(sc, a);
 }
 
 size_t order_scratch_bytes(int64_t n) {
@@ -139,7 +226,7 @@ size_t order_scratch_bytes(int64_t n) {
 
 void order_photons_launch(unsigned long long* keys, const float* raw, int n,
                           int key_bits, float* out, void* scratch,
-                          cudaStream_t st) {
+                          cudaStream_t st, uint32_t* first) {
   if (n <= 0) return;
   unsigned long long* kb = (unsigned long long*)scratch;
   uint32_t* va = (uint32_t*)(kb + n);
@@ -151,6 +238,7 @@ void order_photons_launch(unsigned long long* keys, const float* raw, int n,
   const bool in_b = radix_sort_pairs<unsigned long long>(keys, va, kb, vb, n,
                                                           key_bits, hist, st);
   gather_photons_kernel<<<gb, tb, 0, st>>>(raw, in_b ? vb : va, n, out);
+  if (first) first_of_photon_kernel<<<gb, tb, 0, st>>>(in_b ? kb : keys, n, first);
 }
 
 }  // namespace pm
