@@ -53,6 +53,7 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-render", action="store_true", help="skip the render-rate measurements")
+    ap.add_argument("--no-grad", action="store_true", help="skip the gradient measurements")
     ap.add_argument("--convergence", type=int, nargs="*", default=None, metavar="CONFIG",
                     help="instead of the benchmark: image error against the path tracer for "
                          "these configs (default 1 2 3), beside the reference integrator's")
@@ -268,6 +269,78 @@ def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
     return out
 
 
+# ------------------------------------------------------------------ gradients
+
+# the config-1 Cornell box at 256^2, 1M photons, k = 50, final
+# gathering, 16 spp; loss = MSE against a render with seed-perturbed albedos
+# (8 materials x RGB) and emission
+GRAD_CONFIG = dict(width=256, height=256, spp=16, photons=1_000_000, k=50, fg=1, n_gather=1)
+GRAD_STEPS = 5
+
+
+def gradient_rates(ctx, mesh, camera, dev) -> dict:
+    """Gradient evaluations per second (forward render + device adjoint,
+    photon maps traced in every evaluation) against the plain per-scene
+    loop (PhotonMapping.build + render) on the same setting, and central
+    finite differences (decisions frozen) of 4 parameter channels against
+    the adjoint at full size."""
+    import torch
+    from photon_mapping_b200 import differentiable as D
+    from photon_mapping_b200.integrator import PhotonMapping
+    c = GRAD_CONFIG
+    r = D.DiffRenderer(ctx, mesh, camera, c["width"], c["height"], c["spp"], c["photons"],
+                       c["k"], final_gathering_depth=c["fg"], max_depth=MAX_DEPTH,
+                       n_gather=c["n_gather"], seed=TRACE_SEED)
+    a0, e0 = r.base()
+    ta, te = D.perturbed_parameters(a0, e0, seed=0)
+    target = r.forward(ta, te).astype(np.float64)
+    for _ in range(2):
+        r.loss_and_grad(a0, e0, target)
+    torch.cuda.synchronize(dev)
+    t_fwd, t_bwd = [], []
+    for _ in range(GRAD_STEPS):
+        t0 = time.perf_counter()
+        img = r.forward(a0, e0)
+        t1 = time.perf_counter()
+        diff = img.astype(np.float64) - target
+        loss = float(np.mean(diff * diff))
+        ga, ge = r.backward((2.0 / diff.size) * diff)
+        t2 = time.perf_counter()
+        t_fwd.append(t1 - t0)
+        t_bwd.append(t2 - t1)
+    grad_s = (sum(t_fwd) + sum(t_bwd)) / GRAD_STEPS
+    pmi = PhotonMapping(c["photons"], c["k"], 1.0, c["k"], c["fg"], MAX_DEPTH, ctx=ctx)
+    pmi.build(r.scene, seed=TRACE_SEED)
+    plain, _ = pmi.render(camera, c["width"], c["height"], c["spp"], n_gather=c["n_gather"])
+    t_plain = []
+    for _ in range(GRAD_STEPS):
+        t0 = time.perf_counter()
+        pmi.build(r.scene, seed=TRACE_SEED)
+        pmi.render(camera, c["width"], c["height"], c["spp"], n_gather=c["n_gather"])
+        t_plain.append(time.perf_counter() - t0)
+    plain_s = sum(t_plain) / GRAD_STEPS
+    which = [(2, 0), (3, 1), (6, 2), (len(a0), 0)]   # floor R, leftWall G, shortBox B, Le R
+    fd = r.finite_differences(a0, e0, target, h=1e-3, which=which)
+    g = np.concatenate([ga, ge[None]])
+    fd_err = max(abs(g[p, ch] - fd[p, ch]) / max(abs(fd[p, ch]), 1e-30) for p, ch in which)
+    return {
+        "workload": ("configs[3]: Cornell box (8 material albedos x RGB + emission RGB = 27 "
+                     f"parameters), {c['width']}x{c['height']}, {c['spp']} spp, "
+                     f"{c['photons']} photons, k={c['k']}, final gathering; MSE loss against "
+                     "a render with seed-perturbed parameters"),
+        "grad_evals_per_s": 1.0 / grad_s,
+        "forward_s": sum(t_fwd) / GRAD_STEPS,
+        "backward_s": sum(t_bwd) / GRAD_STEPS,
+        "plain_evals_per_s": 1.0 / plain_s,
+        "grad_vs_plain": plain_s / grad_s,
+        "image_rmse_vs_plain": float(np.sqrt(np.mean((img.astype(np.float64) - plain) ** 2))),
+        "loss": loss,
+        "fd_check": {"channels": which, "h": 1e-3, "max_rel_err": fd_err},
+        "timing": "host wall clock per evaluation (photon trace + map build + render "
+                  "[+ adjoint]), inputs and image on the host",
+    }
+
+
 # -------------------------------------------------------------------- our arm
 
 def run_ours(args) -> None:
@@ -378,6 +451,8 @@ def run_ours(args) -> None:
     render = {} if args.no_render else render_rates(
         ctx, sc, mesh, camera, dev, cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
 
+    grad = None if args.no_grad else gradient_rates(ctx, mesh, camera, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = cpu_reference_rate(photons, queries, CPU_SAMPLE_QUERIES)
@@ -419,6 +494,7 @@ def run_ours(args) -> None:
                          "seconds": trace_s, "photons_per_s": N_EMIT / trace_s,
                          "includes": "emission, tracing, ordering and the map build"},
         "render": render,
+        "gradient": grad,
         "clocks": clk,
         "wall_s_timed_region": t_wall,
     }
