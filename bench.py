@@ -54,6 +54,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-render", action="store_true", help="skip the render-rate measurements")
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient measurements")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-render measurements")
+    ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--convergence", type=int, nargs="*", default=None, metavar="CONFIG",
                     help="instead of the benchmark: image error against the path tracer for "
                          "these configs (default 1 2 3), beside the reference integrator's")
@@ -341,6 +343,71 @@ def gradient_rates(ctx, mesh, camera, dev) -> dict:
     }
 
 
+# ------------------------------------------------------------- batched render
+
+BATCH_STEPS = 3
+
+
+def batched_rates(n_scenes: int, dev) -> dict:
+    """n_scenes random scenes rendered as one batch (one step =
+    every scene's photon trace, map build, camera pass, kNN estimates and
+    resolve; CUDA graph, autotuned launch shapes) against the per-scene
+    sequential loop over the same scenes; the images must be identical."""
+    import torch
+    from photon_mapping_b200 import batch as B
+    scenes = [B.random_scene(1000 + s) for s in range(n_scenes)]
+    samples = sum(sc["width"] * sc["height"] * sc["spp"] for sc in scenes)
+    seq = B.Sequential(scenes)
+    seq.render()                                   # warm-up
+    seq_s = []
+    for _ in range(BATCH_STEPS):
+        imgs, secs = seq.render()
+        seq_s.append(secs)
+    seq.close()
+    del seq
+    torch.cuda.synchronize(dev)
+    br = B.BatchRenderer(scenes)
+    t0 = time.perf_counter()
+    best, stage_ms = br.autotune()
+    tune_s = time.perf_counter() - t0
+    br.render(use_graph=True)                      # capture + warm-up
+    br.render(use_graph=True)
+    dev_ms, wall_s = [], []
+    for _ in range(BATCH_STEPS):
+        t0 = time.perf_counter()
+        dev_ms.append(br.render(use_graph=True))
+        wall_s.append(time.perf_counter() - t0)
+    nograph_ms = br.render(use_graph=False)
+    max_diff = max(float(np.abs(br.image(i) - imgs[i]).max()) for i in range(n_scenes))
+    stored, queries = br.counts()
+    br.close()
+    step_s = sum(wall_s) / len(wall_s)
+    seq_step = sum(seq_s) / len(seq_s)
+    tris = [sc["mesh"].n_faces for sc in scenes]
+    return {
+        "workload": (f"configs[4]: {n_scenes} random Cornell variants (1-40 boxes, displaced "
+                     "heightfield floor, triangles log-uniform 1k-500k), photons log-uniform "
+                     "100k-4M, k in {50,100}, square images side log-uniform 128-1024, "
+                     f"{scenes[0]['spp']} spp, photon-map estimate at the first diffuse hit"),
+        "scenes": n_scenes,
+        "triangles": {"min": min(tris), "max": max(tris), "total": sum(tris)},
+        "photons_emitted": sum(sc["photons"] for sc in scenes),
+        "photons_stored": int(stored.sum()),
+        "queries": int(queries.sum()),
+        "samples_per_step": samples,
+        "batched": {"step_ms_device": sum(dev_ms) / len(dev_ms), "step_s_wall": step_s,
+                    "samples_per_s": samples / step_s, "scenes_per_s": n_scenes / step_s,
+                    "step_ms_without_graph": nograph_ms},
+        "sequential": {"step_s_wall": seq_step, "samples_per_s": samples / seq_step,
+                       "scenes_per_s": n_scenes / seq_step},
+        "batched_vs_sequential": seq_step / step_s,
+        "max_abs_image_difference": max_diff,
+        "tuning": best,
+        "tuned_stage_ms": {"trace": stage_ms[0], "camera": stage_ms[1], "knn": stage_ms[2]},
+        "autotune_s": tune_s,
+    }
+
+
 # -------------------------------------------------------------------- our arm
 
 def run_ours(args) -> None:
@@ -452,6 +519,7 @@ def run_ours(args) -> None:
         ctx, sc, mesh, camera, dev, cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
 
     grad = None if args.no_grad else gradient_rates(ctx, mesh, camera, dev)
+    batched = None if args.no_batch else batched_rates(args.batch_scenes, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -495,6 +563,7 @@ def run_ours(args) -> None:
                          "includes": "emission, tracing, ordering and the map build"},
         "render": render,
         "gradient": grad,
+        "batched": batched,
         "clocks": clk,
         "wall_s_timed_region": t_wall,
     }

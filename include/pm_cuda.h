@@ -364,6 +364,74 @@ int pm_diff_forward(pm_ctx* ctx, const pm_camera* camera,
 int pm_diff_backward(pm_ctx* ctx, const float* grad_rgb, float* grad_albedo,
                      float* grad_emission);
 
+/* ------------------------------------------------------- batched render
+ * Many scenes, views and query sets of uneven size rendered together. The
+ * reference renders one scene per process (examples/main.cpp:7-71:
+ * Scene::loadModel, PhotonMapping::build, the OpenMP pixel loop over
+ * integrate); a batch runs that for every scene at once. One step traces
+ * the global photon map of every scene (one launch), orders and builds each
+ * map (per scene, on 8 streams), runs the camera pass of every pixel of
+ * every scene (one launch), and answers every photon-map query of every
+ * scene in one persistent kNN launch, then resolves every image (one
+ * launch). The step can be captured once in a CUDA graph and replayed.
+ *
+ * The render of scene s is the one pm_photons_trace + pm_render give on
+ * its own context for the same scene, seed, camera and parameters, with
+ * finalGatheringDepth 0 (the estimate at the first diffuse hit) and spp
+ * samples per pixel: the images are identical. */
+
+#define PM_BATCH_MAX_SCENES 256
+
+typedef struct pm_batch pm_batch;
+
+typedef struct pm_batch_scene {
+  const float* vertices;          /* as pm_scene_upload; read during create */
+  const float* normals;
+  const pm_material* materials;
+  int64_t n_faces;
+  pm_camera camera;
+  int32_t width, height, spp;
+  int32_t k;                      /* nEstimationGlobal                     */
+  int32_t max_depth;              /* maxDepth                              */
+  int32_t reserved;
+  int64_t n_photons;              /* nPhotonsGlobal                        */
+  uint64_t seed;                  /* pm_photons_trace seed                 */
+} pm_batch_scene;
+
+/* Launch shapes of the batched kernels (pm_batch_autotune picks them). */
+typedef struct pm_batch_tuning {
+  int32_t knn_warps;   /* warps per block of the persistent kNN kernel, 1..8 */
+  int32_t knn_chunk;   /* consecutive queries per warp work item, 1..1024    */
+  int32_t knn_buffer;  /* candidate buffer per warp: 512 (k <= 224) or 2048  */
+  int32_t bvh_stack;   /* BVH traversal stack entries: 32 or 64              */
+  int32_t block;       /* threads per block of trace and camera: 64..256     */
+  int32_t reserved;
+} pm_batch_tuning;
+
+/* Uploads every scene (its own LBVH), sizes every buffer by running the
+ * step once (photons stored and queries per scene), and keeps the scenes'
+ * parameters. */
+int pm_batch_create(int device, const pm_batch_scene* scenes, int32_t n_scenes,
+                    pm_batch** out);
+int pm_batch_destroy(pm_batch* batch);
+const char* pm_batch_last_error(const pm_batch* batch);
+int pm_batch_set_tuning(pm_batch* batch, const pm_batch_tuning* tuning);
+int pm_batch_get_tuning(pm_batch* batch, pm_batch_tuning* tuning);
+/* Times candidate launch shapes on this batch's own work (trace and camera
+ * kernels: block x stack depth; kNN: warps x chunk x buffer), keeps the
+ * fastest that reported no error, and returns it. ms_per_stage (may be
+ * NULL) receives the best times of {trace, camera, kNN} in ms. */
+int pm_batch_autotune(pm_batch* batch, pm_batch_tuning* best, float* ms_per_stage);
+/* One step over every scene. use_graph != 0: the step is captured in a
+ * CUDA graph on first use (and after a tuning change) and replayed. ms
+ * (may be NULL) receives the step's device time. */
+int pm_batch_render(pm_batch* batch, int32_t use_graph, float* ms);
+/* Image of scene s after the last step: height x width x 3 floats. */
+int pm_batch_image(pm_batch* batch, int32_t scene, float* out_rgb);
+/* Photons stored and photon-map queries answered per scene (n_scenes each;
+ * either may be NULL). */
+int pm_batch_counts(pm_batch* batch, int64_t* photons_stored, int64_t* queries);
+
 #ifdef __cplusplus
 }
 #endif

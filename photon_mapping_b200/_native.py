@@ -71,6 +71,15 @@ _SIGNATURES = {
     "pm_diff_set_parameters": (C.c_int, [_vp, _vp, _i64, C.c_int32]),
     "pm_diff_forward": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "pm_diff_backward": (C.c_int, [_vp, _vp, _vp, _vp]),
+    "pm_batch_create": (C.c_int, [C.c_int, _vp, C.c_int32, C.POINTER(_vp)]),
+    "pm_batch_destroy": (C.c_int, [_vp]),
+    "pm_batch_last_error": (C.c_char_p, [_vp]),
+    "pm_batch_set_tuning": (C.c_int, [_vp, _vp]),
+    "pm_batch_get_tuning": (C.c_int, [_vp, _vp]),
+    "pm_batch_autotune": (C.c_int, [_vp, _vp, _vp]),
+    "pm_batch_render": (C.c_int, [_vp, C.c_int32, _vp]),
+    "pm_batch_image": (C.c_int, [_vp, C.c_int32, _vp]),
+    "pm_batch_counts": (C.c_int, [_vp, _vp, _vp]),
 }
 
 

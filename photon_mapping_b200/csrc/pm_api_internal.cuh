@@ -81,6 +81,21 @@ struct DiffState {
   }
 };
 
+inline SceneDev scene_view(const DevScene& scene, int* err) {
+  SceneDev v;
+  v.tri = (const float4*)scene.tri.ptr;
+  v.nrm = (const float4*)scene.nrm.ptr;
+  v.geo = (const float4*)scene.geo.ptr;
+  v.mat = (const Material*)scene.mat.ptr;
+  v.lights = (const int*)scene.lights.ptr;
+  v.mt = (const float4*)scene.mt.ptr;
+  v.nodes = (const float4*)scene.nodes.ptr;
+  v.n_faces = (int)scene.n_faces;
+  v.n_lights = scene.n_lights;
+  v.err = err;
+  return v;
+}
+
 // Work counters: each kNN launch takes the next slot of a ring, so launches
 // in flight on different streams do not share a counter (up to kCounterRing
 // launches in flight at once).
@@ -132,20 +147,7 @@ struct pm_ctx {
     r_res.release(); r_sort.release(); r_misc.release();
     diff.release();
   }
-  pm::SceneDev scene_view() const {
-    pm::SceneDev v;
-    v.tri = (const float4*)scene.tri.ptr;
-    v.nrm = (const float4*)scene.nrm.ptr;
-    v.geo = (const float4*)scene.geo.ptr;
-    v.mat = (const pm::Material*)scene.mat.ptr;
-    v.lights = (const int*)scene.lights.ptr;
-    v.mt = (const float4*)scene.mt.ptr;
-    v.nodes = (const float4*)scene.nodes.ptr;
-    v.n_faces = (int)scene.n_faces;
-    v.n_lights = scene.n_lights;
-    v.err = (int*)dev_err.ptr;
-    return v;
-  }
+  pm::SceneDev scene_view() const { return pm::scene_view(scene, (int*)dev_err.ptr); }
 };
 
 namespace pm {
@@ -155,6 +157,11 @@ MapDev map_view(const DevMap& dm);
 int build_map(pm_ctx* c, DevMap& dm, const float* d_aos, int64_t n,
               cudaStream_t st);
 int take_device_error(pm_ctx* c, const char* where);
+// Uploads a scene and builds its LBVH on stream st (synchronises st). On
+// failure returns the status and names the step in *what.
+int upload_scene(DevScene& sc, DevBuf& scratch, cudaStream_t st, const float* vertices,
+                 const float* normals, const pm_material* materials, int64_t n,
+                 const char** what);
 // Traces `map` (the body of pm_photons_trace; the caller holds the lock).
 // dmat: decision materials (frozen decisions) or null; first: receives the
 // first stored photon of each emitted photon, or null.

@@ -47,6 +47,71 @@ int take_device_error(pm_ctx* c, const char* where) {
 
 namespace pm {
 
+int upload_scene(DevScene& sc, DevBuf& scratch, cudaStream_t st, const float* vertices,
+                 const float* normals, const pm_material* materials, int64_t n,
+                 const char** what) {
+  sc.built = false;
+  ++sc.generation;
+  // area lights in face order (scene.h:41-51, :245-252)
+  std::vector<int> lights;
+  for (int64_t f = 0; f < n; ++f)
+    if (materials[f].le[0] > 0.f || materials[f].le[1] > 0.f ||
+        materials[f].le[2] > 0.f)
+      lights.push_back((int)f);
+  sc.n_faces = n;
+  sc.n_lights = (int)lights.size();
+  sc.has_specular = false;
+  for (int a = 0; a < 3; ++a) {
+    sc.lo[a] = n > 0 ? vertices[a] : 0.f;
+    sc.hi[a] = sc.lo[a];
+  }
+  for (int64_t f = 0; f < n; ++f) {
+    sc.has_specular |= materials[f].type != PM_LAMBERT;
+    for (int k = 0; k < 3; ++k)
+      for (int a = 0; a < 3; ++a) {
+        const float x = vertices[9 * f + 3 * k + a];
+        if (x < sc.lo[a]) sc.lo[a] = x;
+        if (x > sc.hi[a]) sc.hi[a] = x;
+      }
+  }
+  if (n == 0) {
+    sc.built = true;
+    return PM_OK;
+  }
+  const size_t nf = (size_t)n;
+  int s;
+  *what = "scene allocation";
+  if ((s = sc.verts_in.ensure(nf * 9 * 4)) || (s = sc.nrms_in.ensure(nf * 9 * 4)) ||
+      (s = sc.tri.ensure(nf * 3 * 16)) || (s = sc.nrm.ensure(nf * 3 * 16)) ||
+      (s = sc.geo.ensure(nf * 16)) || (s = sc.mat.ensure(nf * sizeof(Material))) ||
+      (s = sc.lights.ensure((lights.size() + 1) * 4)) ||
+      (s = sc.mt.ensure(nf * 3 * 16)) ||
+      (s = sc.nodes.ensure((nf > 1 ? nf - 1 : 1) * 4 * 16)) ||
+      (s = scratch.ensure(scene_build_scratch_bytes((int)n))))
+    return s;
+  cudaError_t e;
+  *what = "scene upload";
+  if ((e = cudaMemcpyAsync(sc.verts_in.ptr, vertices, nf * 9 * 4,
+                           cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(sc.nrms_in.ptr, normals, nf * 9 * 4,
+                           cudaMemcpyHostToDevice, st)) ||
+      (e = cudaMemcpyAsync(sc.mat.ptr, materials, nf * sizeof(Material),
+                           cudaMemcpyHostToDevice, st)) ||
+      (!lights.empty() &&
+       (e = cudaMemcpyAsync(sc.lights.ptr, lights.data(), lights.size() * 4,
+                            cudaMemcpyHostToDevice, st))))
+    return e == cudaErrorMemoryAllocation ? PM_ERR_OUT_OF_MEMORY : PM_ERR_CUDA;
+  scene_build_launch((const float*)sc.verts_in.ptr, (const float*)sc.nrms_in.ptr,
+                     (int)n, (float4*)sc.tri.ptr, (float4*)sc.nrm.ptr,
+                     (float4*)sc.geo.ptr, (float4*)sc.mt.ptr,
+                     (float4*)sc.nodes.ptr, scratch.ptr, st);
+  *what = "scene build";
+  if ((e = cudaGetLastError()) != cudaSuccess) return PM_ERR_CUDA;
+  if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return PM_ERR_CUDA;
+  sc.built = true;
+  return PM_OK;
+}
+
 int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
               const Material* dmat, DevBuf* first, pm_trace_stats* stats) {
   c->diff.ready = false;  // the photon maps are about to change
@@ -138,67 +203,15 @@ int pm_scene_upload(pm_ctx* c, const float* vertices, const float* normals,
                      (long long)f, materials[f].type);
   std::lock_guard<std::mutex> lk(c->mu);
   cudaSetDevice(c->device);
-  DevScene& sc = c->scene;
-  sc.built = false;
-  ++sc.generation;
   int s;
   if ((s = ensure_err(c)) != PM_OK) return set_err(c, s, "error word");
-  // area lights in face order (scene.h:41-51, :245-252)
-  std::vector<int> lights;
-  for (int64_t f = 0; f < n; ++f)
-    if (materials[f].le[0] > 0.f || materials[f].le[1] > 0.f ||
-        materials[f].le[2] > 0.f)
-      lights.push_back((int)f);
-  sc.n_faces = n;
-  sc.n_lights = (int)lights.size();
-  sc.has_specular = false;
-  for (int a = 0; a < 3; ++a) {
-    sc.lo[a] = n > 0 ? vertices[a] : 0.f;
-    sc.hi[a] = sc.lo[a];
+  const char* what = "";
+  if ((s = upload_scene(c->scene, c->scratch, c->stream, vertices, normals, materials, n,
+                        &what)) != PM_OK) {
+    if (s == PM_ERR_CUDA || s == PM_ERR_OUT_OF_MEMORY)
+      cudaGetLastError();
+    return set_err(c, s, "%s (%lld faces)", what, (long long)n);
   }
-  for (int64_t f = 0; f < n; ++f) {
-    sc.has_specular |= materials[f].type != PM_LAMBERT;
-    for (int k = 0; k < 3; ++k)
-      for (int a = 0; a < 3; ++a) {
-        const float x = vertices[9 * f + 3 * k + a];
-        if (x < sc.lo[a]) sc.lo[a] = x;
-        if (x > sc.hi[a]) sc.hi[a] = x;
-      }
-  }
-  if (n == 0) {
-    sc.built = true;
-    return PM_OK;
-  }
-  const size_t nf = (size_t)n;
-  if ((s = sc.verts_in.ensure(nf * 9 * 4)) || (s = sc.nrms_in.ensure(nf * 9 * 4)) ||
-      (s = sc.tri.ensure(nf * 3 * 16)) || (s = sc.nrm.ensure(nf * 3 * 16)) ||
-      (s = sc.geo.ensure(nf * 16)) || (s = sc.mat.ensure(nf * sizeof(Material))) ||
-      (s = sc.lights.ensure((lights.size() + 1) * 4)) ||
-      (s = sc.mt.ensure(nf * 3 * 16)) ||
-      (s = sc.nodes.ensure((nf > 1 ? nf - 1 : 1) * 4 * 16)) ||
-      (s = c->scratch.ensure(scene_build_scratch_bytes((int)n))))
-    return set_err(c, s, "scene allocation (%lld faces)", (long long)n);
-  cudaStream_t st = c->stream;
-  cudaError_t e;
-  if ((e = cudaMemcpyAsync(sc.verts_in.ptr, vertices, nf * 9 * 4,
-                           cudaMemcpyHostToDevice, st)) ||
-      (e = cudaMemcpyAsync(sc.nrms_in.ptr, normals, nf * 9 * 4,
-                           cudaMemcpyHostToDevice, st)) ||
-      (e = cudaMemcpyAsync(sc.mat.ptr, materials, nf * sizeof(Material),
-                           cudaMemcpyHostToDevice, st)) ||
-      (!lights.empty() &&
-       (e = cudaMemcpyAsync(sc.lights.ptr, lights.data(), lights.size() * 4,
-                            cudaMemcpyHostToDevice, st))))
-    return cuda_status(c, e, "scene upload");
-  scene_build_launch((const float*)sc.verts_in.ptr, (const float*)sc.nrms_in.ptr,
-                     (int)n, (float4*)sc.tri.ptr, (float4*)sc.nrm.ptr,
-                     (float4*)sc.geo.ptr, (float4*)sc.mt.ptr,
-                     (float4*)sc.nodes.ptr, c->scratch.ptr, st);
-  if ((e = cudaGetLastError()) != cudaSuccess)
-    return cuda_status(c, e, "scene build");
-  if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
-    return cuda_status(c, e, "scene build");
-  sc.built = true;
   return PM_OK;
 }
 

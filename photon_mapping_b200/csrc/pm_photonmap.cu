@@ -10,6 +10,7 @@
 //                         maxDist2 = largest kept dist2
 //   integrator.h:133-152  radiance estimate with the Lambert BRDF
 //   material.h:80-88      Lambert::evaluate
+#include "pm_batch.cuh"
 #include "pm_photonmap.cuh"
 #include "pm_sort.cuh"
 
@@ -712,6 +713,206 @@ __device__ __forceinline__ float cold_tau(const float4* pos4, const float4* boxe
   return __uint_as_float(kth_key);
 }
 
+// Answers queries [qb, qe) of a work item on map m, one at a time (one warp).
+// r_hint: the last exact k-th distance this warp found (in/out).
+template <int C, int MODE, bool S>
+__device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, WarpBuf<C>& s,
+                                          int lane, const void* __restrict__ queries,
+                                          int64_t qb, int64_t qe, int k, float n_emitted,
+                                          const KnnOut& out, const uint32_t* __restrict__ order,
+                                          int stride4, float& r_hint) {
+  const float kInf = __int_as_float(0x7f800000);
+  bool have_prev = false;
+  float pqx = 0.f, pqy = 0.f, pqz = 0.f, pkth = 0.f;
+  for (int64_t qi = qb; qi < qe; ++qi) {
+    Query q;
+    q.k = k;
+    q.cnt = 0;
+    q.tau = kInf;
+    const int64_t rec = (MODE != kModeKnn && order) ? (int64_t)__ldg(order + qi) : qi;
+    if (MODE != kModeKnn) {
+      // radiance record r0 = {pos, rho.r}; wo, ns and the other albedo
+      // channels are read after the search
+      const float4 r0 =
+          __ldg(reinterpret_cast<const float4*>(queries) + stride4 * rec);
+      q.x = r0.x; q.y = r0.y; q.z = r0.z;
+    } else {
+      const float* q3 = reinterpret_cast<const float*>(queries) + 3 * qi;
+      q.x = __ldg(q3);
+      q.y = __ldg(q3 + 1);
+      q.z = __ldg(q3 + 2);
+    }
+
+    const bool bad = m.n == 0 || isnan(q.x) || isnan(q.y) || isnan(q.z);
+    if (!bad) {
+      bool warm = false;
+      if (have_prev) {
+        const float d2 = dist2_ref(q.x, q.y, q.z, pqx, pqy, pqz);
+        if (d2 <= pkth) {
+          const float r = sqrtf(pkth) + sqrtf(d2);
+          const float rr = r * 1.00001f;
+          q.tau = fmaxf(rr * rr * 1.00001f, 1e-37f);
+          warm = true;
+        }
+      }
+      // Guess and verify when no bound is known: collect with a radius a
+      // little above the last k-th distance this warp found; k photons or
+      // more inside it make the result exact, otherwise the radius
+      // doubles (twice), then the patch bound of cold_tau is used.
+      bool guess = false, need_cold = false;
+      float rg = 0.f;
+      if (!warm) {
+        stat_add<S>(s, lane, kStatCold, 1);
+        if (r_hint > 0.f) {
+          guess = true;
+          rg = 1.3f * r_hint;
+          q.tau = fmaxf(rg * rg, 1e-37f);
+        } else {
+          need_cold = true;
+        }
+      }
+      for (int attempt = 0;; ++attempt) {
+        if (need_cold) {
+          q.tau = cold_tau<C, S>(m.pos4, m.boxes, m.n, m.nlevels, &L, q.x, q.y,
+                                 q.z, k, &s, lane);
+          need_cold = false;
+          guess = false;
+        }
+        collect<C, S>(m, L, q, s, lane);
+        if (!guess || q.cnt >= k) break;
+        if (attempt < 2) {
+          rg *= 2.0f;
+          q.tau = fmaxf(rg * rg, 1e-37f);
+        } else {
+          need_cold = true;
+        }
+      }
+    }
+    __syncwarp();
+    stat_add<S>(s, lane, kStatQueries, 1);
+    stat_add<S>(s, lane, kStatCand, (uint32_t)q.cnt);
+    const int cnt = q.cnt;
+
+    // final selection
+    const bool all = cnt <= k;
+    uint32_t kth_key = 0, kth_oid = 0xffffffffu;
+    if (all) {
+      uint32_t mx = 0;
+      for (int i = lane; i < cnt; i += 32) mx = max(mx, s.key[i]);
+      kth_key = __reduce_max_sync(kFull, mx);
+    } else {
+      select_kth<C, S>(m.pos4, s, cnt, k, q.tau, lane, kth_key, kth_oid);
+    }
+    const int kept = all ? cnt : k;
+    const float maxd2 = kept > 0 ? __uint_as_float(kth_key) : 0.f;
+
+    if (MODE == kModeAdjoint) {
+      // d estimate / d throughput_i = f(wo, wi_i) / (n_emitted pi maxd2)
+      // for the kept photons (integrator.h:141-150)
+      const float4* q4 =
+          reinterpret_cast<const float4*>(queries) + stride4 * rec;
+      const float4 r0 = __ldg(q4);
+      const float4 r1 = __ldg(q4 + 1);
+      const float4 r2 = __ldg(q4 + 2);
+      const float ax = out.adj_in[3 * rec], ay = out.adj_in[3 * rec + 1],
+                  az = out.adj_in[3 * rec + 2];
+      const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
+      if (kept > 0 && (ax != 0.f || ay != 0.f || az != 0.f)) {
+        const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
+        const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
+        const float cr = __fdiv_rn(__fmul_rn(ax, __fdiv_rn(r0.w, kPI)), den);
+        const float cg = __fdiv_rn(__fmul_rn(ay, __fdiv_rn(r1.w, kPI)), den);
+        const float cb = __fdiv_rn(__fmul_rn(az, __fdiv_rn(r2.w, kPI)), den);
+        for (int i = lane; i < nk; i += 32) {
+          const uint32_t id = s.id[i];
+          const float4 t = __ldg(m.thr4 + id);
+          const float2 w = __ldg(m.wi2 + id);
+          const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
+          if (!(cos_o < 0.f) && !(cos_i < 0.f))
+            atomicAdd(out.photon_adj + orig_index(m.pos4, id), make_float4(cr, cg, cb, 0.f));
+        }
+      }
+    } else if (MODE == kModeRadiance) {
+      // r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b}
+      const float4* q4 =
+          reinterpret_cast<const float4*>(queries) + stride4 * rec;
+      const float4 r0 = __ldg(q4);
+      const float4 r1 = __ldg(q4 + 1);
+      const float4 r2 = __ldg(q4 + 2);
+      const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
+      const float fr = __fdiv_rn(r0.w, kPI);
+      const float fg = __fdiv_rn(r1.w, kPI);
+      const float fb = __fdiv_rn(r2.w, kPI);
+      // the kept entries, in the walk's order whatever the bound was, so
+      // the sum below does not depend on the order queries are answered
+      const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
+      float lr = 0.f, lg = 0.f, lb = 0.f;
+      for (int i = lane; i < nk; i += 32) {
+        const uint32_t id = s.id[i];
+        {
+          const float4 t = __ldg(m.thr4 + id);
+          const float2 w = __ldg(m.wi2 + id);
+          const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
+          // Lambert::evaluate returns 0 when either cosine is < 0
+          if (!(cos_o < 0.f) && !(cos_i < 0.f)) {
+            lr = __fadd_rn(lr, __fmul_rn(fr, t.x));
+            lg = __fadd_rn(lg, __fmul_rn(fg, t.y));
+            lb = __fadd_rn(lb, __fmul_rn(fb, t.z));
+          }
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        lr = __fadd_rn(lr, __shfl_xor_sync(kFull, lr, o));
+        lg = __fadd_rn(lg, __shfl_xor_sync(kFull, lg, o));
+        lb = __fadd_rn(lb, __shfl_xor_sync(kFull, lb, o));
+      }
+      if (lane == 0) {
+        float3 o3 = make_float3(0.f, 0.f, 0.f);
+        if (kept > 0) {
+          const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
+          o3 = make_float3(__fdiv_rn(lr, den), __fdiv_rn(lg, den),
+                           __fdiv_rn(lb, den));
+        }
+        out.rgb[3 * rec + 0] = o3.x;
+        out.rgb[3 * rec + 1] = o3.y;
+        out.rgb[3 * rec + 2] = o3.z;
+      }
+    } else {
+      int n2 = cnt;
+      if (!all) n2 = compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
+      for (int i = lane; i < n2; i += 32)
+        s.id[i] = orig_index(m.pos4, s.id[i]);
+      __syncwarp();
+      int32_t* orow = out.idx + qi * (int64_t)k;
+      for (int i = lane; i < n2; i += 32) {
+        const uint32_t ki = s.key[i], oi = s.id[i];
+        int rank = 0;
+        for (int j = 0; j < n2; ++j) {
+          const uint32_t kj = s.key[j], oj = s.id[j];
+          rank += (kj > ki) || (kj == ki && oj > oi);
+        }
+        orow[rank] = (int32_t)oi;
+      }
+      for (int r = n2 + lane; r < k; r += 32) orow[r] = -1;
+      if (lane == 0) {
+        out.count[qi] = n2;
+        out.maxd2[qi] = maxd2;
+      }
+    }
+    __syncwarp();
+
+    if (!bad && kept >= k) {
+      have_prev = true;
+      pqx = q.x; pqy = q.y; pqz = q.z;
+      pkth = maxd2;
+      r_hint = sqrtf(maxd2);
+    } else {
+      have_prev = false;
+    }
+  }
+}
+
 template <int C, int MODE, bool S>
 __global__ void __launch_bounds__(256, 4)
     knn_kernel(MapDev m, const void* __restrict__ queries, int64_t nq, int k,
@@ -722,7 +923,6 @@ __global__ void __launch_bounds__(256, 4)
   __shared__ Levels L;
   WarpBuf<C>& s = reinterpret_cast<WarpBuf<C>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  const float kInf = __int_as_float(0x7f800000);
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int i = 0; i < kMaxLevels; ++i) {  // constant indices: m stays in
@@ -742,195 +942,8 @@ __global__ void __launch_bounds__(256, 4)
     if (qb >= nq) break;
     const int64_t qe = min(nq, qb + kChunk);
 
-    bool have_prev = false;
-    float pqx = 0.f, pqy = 0.f, pqz = 0.f, pkth = 0.f;
-    for (int64_t qi = qb; qi < qe; ++qi) {
-      Query q;
-      q.k = k;
-      q.cnt = 0;
-      q.tau = kInf;
-      const int64_t rec = (MODE != kModeKnn && order) ? (int64_t)__ldg(order + qi) : qi;
-      if (MODE != kModeKnn) {
-        // radiance record r0 = {pos, rho.r}; wo, ns and the other albedo
-        // channels are read after the search
-        const float4 r0 =
-            __ldg(reinterpret_cast<const float4*>(queries) + stride4 * rec);
-        q.x = r0.x; q.y = r0.y; q.z = r0.z;
-      } else {
-        const float* q3 = reinterpret_cast<const float*>(queries) + 3 * qi;
-        q.x = __ldg(q3);
-        q.y = __ldg(q3 + 1);
-        q.z = __ldg(q3 + 2);
-      }
-
-      const bool bad = m.n == 0 || isnan(q.x) || isnan(q.y) || isnan(q.z);
-      if (!bad) {
-        bool warm = false;
-        if (have_prev) {
-          const float d2 = dist2_ref(q.x, q.y, q.z, pqx, pqy, pqz);
-          if (d2 <= pkth) {
-            const float r = sqrtf(pkth) + sqrtf(d2);
-            const float rr = r * 1.00001f;
-            q.tau = fmaxf(rr * rr * 1.00001f, 1e-37f);
-            warm = true;
-          }
-        }
-        // Guess and verify when no bound is known: collect with a radius a
-        // little above the last k-th distance this warp found; k photons or
-        // more inside it make the result exact, otherwise the radius
-        // doubles (twice), then the patch bound of cold_tau is used.
-        bool guess = false, need_cold = false;
-        float rg = 0.f;
-        if (!warm) {
-          stat_add<S>(s, lane, kStatCold, 1);
-          if (r_hint > 0.f) {
-            guess = true;
-            rg = 1.3f * r_hint;
-            q.tau = fmaxf(rg * rg, 1e-37f);
-          } else {
-            need_cold = true;
-          }
-        }
-        for (int attempt = 0;; ++attempt) {
-          if (need_cold) {
-            q.tau = cold_tau<C, S>(m.pos4, m.boxes, m.n, m.nlevels, &L, q.x, q.y,
-                                   q.z, k, &s, lane);
-            need_cold = false;
-            guess = false;
-          }
-          collect<C, S>(m, L, q, s, lane);
-          if (!guess || q.cnt >= k) break;
-          if (attempt < 2) {
-            rg *= 2.0f;
-            q.tau = fmaxf(rg * rg, 1e-37f);
-          } else {
-            need_cold = true;
-          }
-        }
-      }
-      __syncwarp();
-      stat_add<S>(s, lane, kStatQueries, 1);
-      stat_add<S>(s, lane, kStatCand, (uint32_t)q.cnt);
-      const int cnt = q.cnt;
-
-      // final selection
-      const bool all = cnt <= k;
-      uint32_t kth_key = 0, kth_oid = 0xffffffffu;
-      if (all) {
-        uint32_t mx = 0;
-        for (int i = lane; i < cnt; i += 32) mx = max(mx, s.key[i]);
-        kth_key = __reduce_max_sync(kFull, mx);
-      } else {
-        select_kth<C, S>(m.pos4, s, cnt, k, q.tau, lane, kth_key, kth_oid);
-      }
-      const int kept = all ? cnt : k;
-      const float maxd2 = kept > 0 ? __uint_as_float(kth_key) : 0.f;
-
-      if (MODE == kModeAdjoint) {
-        // d estimate / d throughput_i = f(wo, wi_i) / (n_emitted pi maxd2)
-        // for the kept photons (integrator.h:141-150)
-        const float4* q4 =
-            reinterpret_cast<const float4*>(queries) + stride4 * rec;
-        const float4 r0 = __ldg(q4);
-        const float4 r1 = __ldg(q4 + 1);
-        const float4 r2 = __ldg(q4 + 2);
-        const float ax = out.adj_in[3 * rec], ay = out.adj_in[3 * rec + 1],
-                    az = out.adj_in[3 * rec + 2];
-        const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
-        if (kept > 0 && (ax != 0.f || ay != 0.f || az != 0.f)) {
-          const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
-          const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
-          const float cr = __fdiv_rn(__fmul_rn(ax, __fdiv_rn(r0.w, kPI)), den);
-          const float cg = __fdiv_rn(__fmul_rn(ay, __fdiv_rn(r1.w, kPI)), den);
-          const float cb = __fdiv_rn(__fmul_rn(az, __fdiv_rn(r2.w, kPI)), den);
-          for (int i = lane; i < nk; i += 32) {
-            const uint32_t id = s.id[i];
-            const float4 t = __ldg(m.thr4 + id);
-            const float2 w = __ldg(m.wi2 + id);
-            const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
-            if (!(cos_o < 0.f) && !(cos_i < 0.f))
-              atomicAdd(out.photon_adj + orig_index(m.pos4, id), make_float4(cr, cg, cb, 0.f));
-          }
-        }
-      } else if (MODE == kModeRadiance) {
-        // r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b}
-        const float4* q4 =
-            reinterpret_cast<const float4*>(queries) + stride4 * rec;
-        const float4 r0 = __ldg(q4);
-        const float4 r1 = __ldg(q4 + 1);
-        const float4 r2 = __ldg(q4 + 2);
-        const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
-        const float fr = __fdiv_rn(r0.w, kPI);
-        const float fg = __fdiv_rn(r1.w, kPI);
-        const float fb = __fdiv_rn(r2.w, kPI);
-        // the kept entries, in the walk's order whatever the bound was, so
-        // the sum below does not depend on the order queries are answered
-        const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
-        float lr = 0.f, lg = 0.f, lb = 0.f;
-        for (int i = lane; i < nk; i += 32) {
-          const uint32_t id = s.id[i];
-          {
-            const float4 t = __ldg(m.thr4 + id);
-            const float2 w = __ldg(m.wi2 + id);
-            const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
-            // Lambert::evaluate returns 0 when either cosine is < 0
-            if (!(cos_o < 0.f) && !(cos_i < 0.f)) {
-              lr = __fadd_rn(lr, __fmul_rn(fr, t.x));
-              lg = __fadd_rn(lg, __fmul_rn(fg, t.y));
-              lb = __fadd_rn(lb, __fmul_rn(fb, t.z));
-            }
-          }
-        }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-          lr = __fadd_rn(lr, __shfl_xor_sync(kFull, lr, o));
-          lg = __fadd_rn(lg, __shfl_xor_sync(kFull, lg, o));
-          lb = __fadd_rn(lb, __shfl_xor_sync(kFull, lb, o));
-        }
-        if (lane == 0) {
-          float3 o3 = make_float3(0.f, 0.f, 0.f);
-          if (kept > 0) {
-            const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
-            o3 = make_float3(__fdiv_rn(lr, den), __fdiv_rn(lg, den),
-                             __fdiv_rn(lb, den));
-          }
-          out.rgb[3 * rec + 0] = o3.x;
-          out.rgb[3 * rec + 1] = o3.y;
-          out.rgb[3 * rec + 2] = o3.z;
-        }
-      } else {
-        int n2 = cnt;
-        if (!all) n2 = compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
-        for (int i = lane; i < n2; i += 32)
-          s.id[i] = orig_index(m.pos4, s.id[i]);
-        __syncwarp();
-        int32_t* orow = out.idx + qi * (int64_t)k;
-        for (int i = lane; i < n2; i += 32) {
-          const uint32_t ki = s.key[i], oi = s.id[i];
-          int rank = 0;
-          for (int j = 0; j < n2; ++j) {
-            const uint32_t kj = s.key[j], oj = s.id[j];
-            rank += (kj > ki) || (kj == ki && oj > oi);
-          }
-          orow[rank] = (int32_t)oi;
-        }
-        for (int r = n2 + lane; r < k; r += 32) orow[r] = -1;
-        if (lane == 0) {
-          out.count[qi] = n2;
-          out.maxd2[qi] = maxd2;
-        }
-      }
-      __syncwarp();
-
-      if (!bad && kept >= k) {
-        have_prev = true;
-        pqx = q.x; pqy = q.y; pqz = q.z;
-        pkth = maxd2;
-        r_hint = sqrtf(maxd2);
-      } else {
-        have_prev = false;
-      }
-    }
+    knn_chunk<C, MODE, S>(m, L, s, lane, queries, qb, qe, k, n_emitted, out, order, stride4,
+                          r_hint);
     if (S) {
       __syncwarp();
       if (lane < 6) {
@@ -995,6 +1008,99 @@ cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                                                out, counter, num_sms, st, order, stride4)
              : launch_one<2048, kModeKnn>(m, queries, nq, k, n_emitted, out,
                                           counter, num_sms, st, order, stride4);
+}
+
+}  // namespace pm
+
+// ------------------------------------------------------------ batched kNN
+namespace pm {
+
+// The radiance estimate of every query of every scene of a batch in one
+// persistent launch. A work item is `chunk` consecutive queries of one
+// scene (in the order of the sorted keys: scene, then Morton code); a warp
+// takes items from `counter` until none are left, switching its copy of the
+// photon map (map pointers, tree shape) when the scene changes.
+template <int C>
+__global__ void __launch_bounds__(256, 4)
+    knn_batch_kernel(BatchTables t, const float4* __restrict__ slots,
+                     const uint32_t* __restrict__ order, const int64_t* __restrict__ qoff,
+                     const int64_t* __restrict__ item_off, int chunk, float* __restrict__ res,
+                     unsigned long long* __restrict__ counter) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ int64_t ioff[kMaxBatchScenes + 1];
+  __shared__ MapDev wmap[8];
+  __shared__ Levels wlev[8];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpBuf<C>& s = reinterpret_cast<WarpBuf<C>*>(smem_raw)[warp];
+  batch_load_offsets(ioff, item_off, t.n_scenes);
+  __syncthreads();
+  const int64_t total = ioff[t.n_scenes];
+  float r_hint = -1.f;
+  int cur = -1, k = 0;
+  float n_emitted = 0.f;
+  KnnOut out{};
+  out.rgb = res;
+  while (true) {
+    unsigned long long c0 = 0;
+    if (lane == 0) c0 = atomicAdd(counter, 1ull);
+    c0 = __shfl_sync(kFull, c0, 0);
+    if ((int64_t)c0 >= total) break;
+    const int sc = batch_find(ioff, t.n_scenes, (int64_t)c0);
+    if (sc != cur) {
+      __syncwarp();
+      if (lane == 0) {
+        const BatchScene& bs = t.scenes[sc];
+        wmap[warp] = bs.map;
+        for (int i = 0; i < kMaxLevels; ++i) {
+          wlev[warp].off[i] = bs.map.lvl_off[i];
+          wlev[warp].cnt[i] = bs.map.lvl_cnt[i];
+        }
+      }
+      __syncwarp();
+      cur = sc;
+      k = t.scenes[sc].k;
+      n_emitted = t.scenes[sc].n_emitted;
+      r_hint = -1.f;
+    }
+    const int64_t qb = qoff[sc] + ((int64_t)c0 - ioff[sc]) * chunk;
+    const int64_t qe = min(qoff[sc + 1], qb + chunk);
+    knn_chunk<C, kModeRadiance, false>(wmap[warp], wlev[warp], s, lane, slots, qb, qe, k,
+                                       n_emitted, out, order, 4, r_hint);
+  }
+}
+
+cudaError_t batch_knn_prepare(int warps, int buffer, int* blocks_per_sm) {
+  if (warps < 1 || warps > 8) return cudaErrorInvalidValue;
+  auto kern = buffer <= 512 ? knn_batch_kernel<512> : knn_batch_kernel<2048>;
+  const size_t smem =
+      (size_t)warps * (buffer <= 512 ? sizeof(WarpBuf<512>) : sizeof(WarpBuf<2048>));
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, smem);
+  if (e != cudaSuccess) return e;
+  *blocks_per_sm = per_sm < 1 ? 1 : per_sm;
+  return cudaSuccess;
+}
+
+cudaError_t batch_knn_launch(const BatchTables& t, const float4* slots, const uint32_t* order,
+                             const int64_t* qoff, const int64_t* item_off, int64_t max_items,
+                             float* res, int warps, int chunk, int buffer, int blocks_per_sm,
+                             unsigned long long* counter, int num_sms, cudaStream_t st) {
+  if (warps < 1 || warps > 8 || chunk < 1) return cudaErrorInvalidValue;
+  const int threads = 32 * warps;
+  auto kern = buffer <= 512 ? knn_batch_kernel<512> : knn_batch_kernel<2048>;
+  const size_t smem =
+      (size_t)warps * (buffer <= 512 ? sizeof(WarpBuf<512>) : sizeof(WarpBuf<2048>));
+  int64_t blocks = (int64_t)num_sms * blocks_per_sm;
+  const int64_t need = (max_items + warps - 1) / warps;
+  if (blocks > need) blocks = need;
+  if (blocks < 1) blocks = 1;
+  cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+  kern<<<(unsigned)blocks, threads, smem, st>>>(t, slots, order, qoff, item_off, chunk, res,
+                                                counter);
+  return cudaGetLastError();
 }
 
 }  // namespace pm

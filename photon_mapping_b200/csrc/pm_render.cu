@@ -16,6 +16,7 @@
 //   3. resolve_kernel, one thread per pixel: per sample in order, direct +
 //      sum(weight * estimate); NaN or negative samples are dropped
 //      (main.cpp:49-56) and the rest added to the pixel.
+#include "pm_batch.cuh"
 #include "pm_photonmap.cuh"
 #include "pm_render.cuh"
 #include "pm_scene.cuh"
@@ -49,6 +50,7 @@ __device__ __forceinline__ void emit_query(const RenderArgs& a, int64_t base,
 }
 
 // PhotonMapping::computeDirectIllumination (integrator.h:178-213).
+template <int STACK>
 __device__ V3 direct_light(const SceneDev& sc, const Surf& s, V3 wo,
                            const Material& m, Rng& rng) {
   float pc, pp;
@@ -58,7 +60,7 @@ __device__ V3 direct_light(const SceneDev& sc, const Surf& s, V3 wo,
   const float r = length(ls.pos - s.pos);
   const float pd = pp * r * r / fabsf(dot(-wi, ls.ns));
   Hit h;
-  if (intersect(sc, s.pos, wi, kRayEps, r - kRayEps, h)) return v3(0.f, 0.f, 0.f);
+  if (intersect_t<STACK>(sc, s.pos, wi, kRayEps, r - kRayEps, h)) return v3(0.f, 0.f, 0.f);
   const Material& lm = sc.mat[lf];
   const V3 le = v3(lm.le[0], lm.le[1], lm.le[2]);
   const V3 f = lambert_eval(m, world_to_local(wo, s.dpdu, s.ns, s.dpdv),
@@ -71,7 +73,7 @@ __device__ V3 direct_light(const SceneDev& sc, const Surf& s, V3 wo,
 // 215-262) for one gather ray: a diffuse hit becomes a global-map query
 // with the accumulated weight, a specular hit continues the path. pid_w is
 // the albedo parameter of the surface the gather starts from.
-template <bool D>
+template <bool D, int STACK>
 __device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
                        const Material* m, V3 w, Rng& rng, int64_t base,
                        int& nq, int pid_w) {
@@ -83,7 +85,7 @@ __device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
     const V3 dir = local_to_world(wi_l, s.dpdu, s.ns, s.dpdv);
     const float c = fabsf(dot(s.ns, dir));
     Hit h;
-    if (!intersect(sc, s.pos, dir, kRayEps, __int_as_float(0x7f7fffff), h)) return;
+    if (!intersect_t<STACK>(sc, s.pos, dir, kRayEps, __int_as_float(0x7f7fffff), h)) return;
     const Surf s2 = surface_at(sc, s.pos, dir, h);
     const Material* m2 = sc.mat + h.prim;
     w = w * (f * c / pdf);
@@ -98,11 +100,9 @@ __device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
   }
 }
 
-template <bool D>
-__global__ void __launch_bounds__(128)
-    camera_kernel(SceneDev sc, RenderArgs a) {
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= a.width * a.height) return;
+// One pixel's samples of the camera pass (all a.batch of them).
+template <bool D, int STACK>
+__device__ __forceinline__ void camera_pixel(const SceneDev& sc, const RenderArgs& a, int p) {
   const int i = p / a.width, j = p % a.width;
   Rng rng{a.rng_state[p]};
   for (int sidx = 0; sidx < a.batch; ++sidx) {
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(128)
       const Frame f = st[--sp];
       if (f.depth >= a.max_depth) continue;
       Hit h;
-      if (!intersect(sc, f.o, f.d, kRayEps, __int_as_float(0x7f7fffff), h)) continue;
+      if (!intersect_t<STACK>(sc, f.o, f.d, kRayEps, __int_as_float(0x7f7fffff), h)) continue;
       const Surf s = surface_at(sc, f.o, f.d, h);
       const Material& m = sc.mat[h.prim];
       const V3 wo = -f.d;
@@ -145,14 +145,14 @@ __global__ void __launch_bounds__(128)
         if (f.depth >= a.fg_depth) {
           emit_query<D>(a, base, nq, kQueryGlobal, s, wo, mat_rho(m), f.w, -1, pid);
         } else {
-          const V3 ld = f.w * direct_light(sc, s, wo, m, rng);
+          const V3 ld = f.w * direct_light<STACK>(sc, s, wo, m, rng);
           direct = direct + ld;
           if (D && nn < a.q_per_sample)
             a.nee[base + nn++] = make_float4(ld.x, ld.y, ld.z, __int_as_float(pid));
           emit_query<D>(a, base, nq, kQueryCaustics, s, wo, mat_rho(m), f.w, -1, pid);
           const V3 wg = f.w * a.inv_gather;
           for (int g = 0; g < a.n_gather; ++g)
-            gather<D>(a, sc, s, wo, &m, wg, rng, base, nq, pid);
+            gather<D, STACK>(a, sc, s, wo, &m, wg, rng, base, nq, pid);
         }
         continue;
       }
@@ -204,6 +204,14 @@ __global__ void __launch_bounds__(128)
     if (D) a.nee_count[srec] = nn;
   }
   a.rng_state[p] = rng.state;
+}
+
+template <bool D>
+__global__ void __launch_bounds__(128)
+    camera_kernel(SceneDev sc, RenderArgs a) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= a.width * a.height) return;
+  camera_pixel<D, kBvhStack>(sc, a, p);
 }
 
 __global__ void rng_init_kernel(unsigned long long* st, int w, int n) {
@@ -262,6 +270,23 @@ __global__ void list_queries_kernel(const float4* __restrict__ slots,
   vals[o] = (uint32_t)t;
 }
 
+// Radiance of sample sidx: direct + sum(weight * estimate) over its slots.
+__device__ __forceinline__ V3 sample_radiance(const float4* __restrict__ slots,
+                                              const float4* __restrict__ srec,
+                                              const float* __restrict__ res, int64_t sidx,
+                                              int q_per_sample) {
+  const float4 d = srec[sidx];
+  V3 rad = v3(d.x, d.y, d.z);
+  const int nq = __float_as_int(d.w);
+  for (int q = 0; q < nq; ++q) {
+    const int64_t t = sidx * q_per_sample + q;
+    const float4 w = slots[4 * t + 3];
+    const V3 l = v3(res[3 * t], res[3 * t + 1], res[3 * t + 2]);
+    rad = rad + v3(w.x, w.y, w.z) * l;
+  }
+  return rad;
+}
+
 __global__ void resolve_kernel(const float4* __restrict__ slots,
                                const float4* __restrict__ srec,
                                const float* __restrict__ res, int npix,
@@ -275,15 +300,7 @@ __global__ void resolve_kernel(const float4* __restrict__ slots,
   unsigned nan_n = 0, neg_n = 0;
   for (int s = 0; s < batch; ++s) {
     const int64_t sidx = (int64_t)p * batch + s;
-    const float4 d = srec[sidx];
-    V3 rad = v3(d.x, d.y, d.z);
-    const int nq = __float_as_int(d.w);
-    for (int q = 0; q < nq; ++q) {
-      const int64_t t = sidx * q_per_sample + q;
-      const float4 w = slots[4 * t + 3];
-      const V3 l = v3(res[3 * t], res[3 * t + 1], res[3 * t + 2]);
-      rad = rad + v3(w.x, w.y, w.z) * l;
-    }
+    const V3 rad = sample_radiance(slots, srec, res, sidx, q_per_sample);
     if (raw) {  // integrate(): the radiance itself, no filtering
       raw[3 * sidx] = rad.x;
       raw[3 * sidx + 1] = rad.y;
@@ -432,6 +449,158 @@ __global__ void __launch_bounds__(128)
 void render_path_tracing(const SceneDev& sc, const PathArgs& a, cudaStream_t s) {
   const int n = a.width * a.height;
   path_trace_kernel<<<(n + 127) / 128, 128, 0, s>>>(sc, a);
+}
+
+}  // namespace pm
+
+// ------------------------------------------------------------ batched pass
+namespace pm {
+
+// Sampler seeds and the camera pass of every pixel of every scene.
+template <int STACK>
+__global__ void __launch_bounds__(256)
+    batch_camera_kernel(BatchTables t, int64_t total) {
+  __shared__ int64_t off[kMaxBatchScenes + 1];
+  batch_load_offsets(off, t.pix_off, t.n_scenes);
+  __syncthreads();
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int s = batch_find(off, t.n_scenes, g);
+  const BatchScene& bs = t.scenes[s];
+  const int p = (int)(g - off[s]);
+  const int i = p / bs.ra.width, j = p % bs.ra.width;
+  bs.ra.rng_state[p] = (unsigned long long)(j + bs.ra.width * i);  // UniformSampler(j + w*i)
+  camera_pixel<false, STACK>(bs.sc, bs.ra, p);
+}
+
+void batch_camera_launch(const BatchTables& t, int64_t total_pix, int block, int stack,
+                         cudaStream_t st) {
+  if (total_pix <= 0) return;
+  const unsigned gb = (unsigned)((total_pix + block - 1) / block);
+  if (stack <= 32)
+    batch_camera_kernel<32><<<gb, block, 0, st>>>(t, total_pix);
+  else
+    batch_camera_kernel<64><<<gb, block, 0, st>>>(t, total_pix);
+}
+
+__global__ void __launch_bounds__(256)
+    batch_list_queries_kernel(BatchTables t, int64_t total, const float4* __restrict__ slots,
+                              unsigned long long* __restrict__ keys,
+                              uint32_t* __restrict__ vals, unsigned* __restrict__ count) {
+  __shared__ int64_t off[kMaxBatchScenes + 1];
+  batch_load_offsets(off, t.slot_off, t.n_scenes);
+  __syncthreads();
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  // every lane reaches the ballot and the shuffle (no early exit)
+  bool mine = false;
+  int s = 0;
+  float4 r0 = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (g < total) {
+    s = batch_find(off, t.n_scenes, g);
+    const BatchScene& bs = t.scenes[s];
+    const int64_t tl = g - off[s];
+    const int64_t sidx = tl / bs.ra.q_per_sample;
+    const int q = (int)(tl % bs.ra.q_per_sample);
+    if (q < __float_as_int(bs.ra.sample_rec[sidx].w)) {
+      mine = __float_as_int(slots[4 * g + 3].w) == kQueryGlobal;
+      r0 = slots[4 * g];
+    }
+  }
+  const unsigned bal = __ballot_sync(kFull, mine);
+  unsigned base = 0;
+  const int leader = bal ? __ffs(bal) - 1 : 0;
+  if (bal && (int)lane_id() == leader) base = atomicAdd(count, (unsigned)__popc(bal));
+  base = __shfl_sync(kFull, base, leader);
+  if (!mine) return;
+  const unsigned o = base + __popc(bal & lanemask_lt());
+  const BatchScene& bs = t.scenes[s];
+  auto cell = [](float v, float l, float ie) -> uint32_t {
+    const float c = (v - l) * ie * 1024.f;
+    if (!(c > 0.f)) return 0u;
+    return c >= 1023.f ? 1023u : (uint32_t)c;
+  };
+  const uint32_t mc = (spread10r(cell(r0.x, bs.qlo.x, bs.qinv.x)) << 2) |
+                      (spread10r(cell(r0.y, bs.qlo.y, bs.qinv.y)) << 1) |
+                      spread10r(cell(r0.z, bs.qlo.z, bs.qinv.z));
+  keys[o] = ((unsigned long long)s << 30) | mc;
+  vals[o] = (uint32_t)g;
+}
+
+void batch_list_queries_launch(const BatchTables& t, int64_t total_slots,
+                               unsigned long long* keys, uint32_t* vals, unsigned* count,
+                               cudaStream_t st) {
+  if (total_slots <= 0) return;
+  batch_list_queries_kernel<<<(unsigned)((total_slots + 255) / 256), 256, 0, st>>>(
+      t, total_slots, t.slots, keys, vals, count);
+}
+
+// Keys past the listed queries are all ones (the list buffer is cleared
+// before listing), so they sort last and name no scene.
+__global__ void batch_query_start_kernel(const unsigned long long* __restrict__ keys, int64_t nq,
+                                         int n, int64_t* __restrict__ qstart) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  const unsigned long long s = keys[i] >> 30;
+  if (s >= (unsigned long long)n) return;
+  if (i == 0 || (keys[i - 1] >> 30) != s) qstart[s] = i;
+}
+
+__global__ void batch_query_prefix_kernel(const int64_t* __restrict__ qstart, int64_t nq,
+                                          const unsigned* __restrict__ listed, int n, int chunk,
+                                          int64_t* __restrict__ qoff,
+                                          int64_t* __restrict__ item_off) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  qoff[n] = min(nq, (int64_t)*listed);
+  for (int s = n - 1; s >= 0; --s) qoff[s] = qstart[s] >= 0 ? qstart[s] : qoff[s + 1];
+  item_off[0] = 0;
+  for (int s = 0; s < n; ++s)
+    item_off[s + 1] = item_off[s] + (qoff[s + 1] - qoff[s] + chunk - 1) / chunk;
+}
+
+void batch_query_ranges_launch(const unsigned long long* sorted_keys, int64_t nq,
+                               const unsigned* listed, int n_scenes, int chunk, int64_t* qstart,
+                               int64_t* qoff, int64_t* item_off, cudaStream_t st) {
+  cudaMemsetAsync(qstart, 0xff, (size_t)n_scenes * sizeof(int64_t), st);
+  if (nq > 0)
+    batch_query_start_kernel<<<(unsigned)((nq + 255) / 256), 256, 0, st>>>(sorted_keys, nq,
+                                                                          n_scenes, qstart);
+  batch_query_prefix_kernel<<<1, 32, 0, st>>>(qstart, nq, listed, n_scenes, chunk, qoff,
+                                              item_off);
+}
+
+__global__ void __launch_bounds__(256) batch_resolve_kernel(BatchTables t, int64_t total) {
+  __shared__ int64_t off[kMaxBatchScenes + 1];
+  batch_load_offsets(off, t.pix_off, t.n_scenes);
+  __syncthreads();
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int s = batch_find(off, t.n_scenes, g);
+  const BatchScene& bs = t.scenes[s];
+  const int p = (int)(g - off[s]);
+  const int batch = bs.ra.batch;
+  float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+  unsigned nan_n = 0, neg_n = 0;
+  for (int k = 0; k < batch; ++k) {
+    const V3 rad = sample_radiance(bs.ra.slots, bs.ra.sample_rec, bs.res,
+                                   (int64_t)p * batch + k, bs.ra.q_per_sample);
+    if (has_nan(rad)) { ++nan_n; continue; }
+    if (rad.x < 0.f || rad.y < 0.f || rad.z < 0.f) { ++neg_n; continue; }
+    acc.x += rad.x;
+    acc.y += rad.y;
+    acc.z += rad.z;
+  }
+  // Image::divide (image.h:49-56)
+  const float spp = (float)(batch > 0 ? batch : 1);
+  bs.image[3 * p] = acc.x / spp;
+  bs.image[3 * p + 1] = acc.y / spp;
+  bs.image[3 * p + 2] = acc.z / spp;
+  if (nan_n) atomicAdd(t.dropped, (unsigned long long)nan_n);
+  if (neg_n) atomicAdd(t.dropped + 1, (unsigned long long)neg_n);
+}
+
+void batch_resolve_launch(const BatchTables& t, int64_t total_pix, cudaStream_t st) {
+  if (total_pix <= 0) return;
+  batch_resolve_kernel<<<(unsigned)((total_pix + 255) / 256), 256, 0, st>>>(t, total_pix);
 }
 
 }  // namespace pm

@@ -94,9 +94,11 @@ __device__ __forceinline__ void test_leaf(const SceneDev& sc, int leaf, V3 o,
 }
 
 // Closest hit with tmin <= t <= tmax; ties in t go to the smaller face id,
-// so the result does not depend on the traversal order.
-__device__ __forceinline__ bool intersect(const SceneDev& sc, V3 o, V3 d,
-                                          float tmin, float tmax, Hit& h) {
+// so the result does not depend on the traversal order. STACK entries of
+// traversal stack (an overflow sets error bit 0 and loses the subtree).
+template <int STACK>
+__device__ __forceinline__ bool intersect_t(const SceneDev& sc, V3 o, V3 d,
+                                            float tmin, float tmax, Hit& h) {
   h.t = tmax;
   h.prim = -1;
   h.u = h.v = 0.f;
@@ -106,7 +108,7 @@ __device__ __forceinline__ bool intersect(const SceneDev& sc, V3 o, V3 d,
     return h.prim >= 0;
   }
   const V3 inv = v3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
-  int stack[kBvhStack];
+  int stack[STACK];
   int sp = 0;
   int node = 0;
   while (true) {
@@ -137,7 +139,7 @@ __device__ __forceinline__ bool intersect(const SceneDev& sc, V3 o, V3 d,
       }
     }
     if (other >= 0) {
-      if (sp < kBvhStack) {
+      if (sp < STACK) {
         stack[sp++] = other;
       } else {
         atomicOr(sc.err, 1);
@@ -151,6 +153,11 @@ __device__ __forceinline__ bool intersect(const SceneDev& sc, V3 o, V3 d,
     }
   }
   return h.prim >= 0;
+}
+
+__device__ __forceinline__ bool intersect(const SceneDev& sc, V3 o, V3 d,
+                                          float tmin, float tmax, Hit& h) {
+  return intersect_t<kBvhStack>(sc, o, d, tmin, tmax, h);
 }
 
 // Surface frame at a hit (scene.h:324-337): position = ray(t), shading

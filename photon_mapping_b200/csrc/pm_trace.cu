@@ -13,6 +13,7 @@
 // Stored photons are appended with an atomic counter and tagged with the
 // key (photon index << 8 | bounce); sorting by that key afterwards gives
 // the order a sequential trace produces.
+#include "pm_batch.cuh"
 #include "pm_scene.cuh"
 #include "pm_sort.cuh"
 #include "pm_trace.cuh"
@@ -55,7 +56,7 @@ struct ReplaySmem {
 
 // One emitted photon of PhotonMapping::build (integrator.h:406-469 global,
 // :483-558 caustics).
-template <int MODE>
+template <int MODE, int STACK>
 __device__ __forceinline__ void trace_one(const SceneDev& sc, const TraceArgs& a, int i,
                                           ReplaySmem* rs) {
   Rng rng{photon_stream_state(a.seed, (unsigned long long)i)};
@@ -93,7 +94,7 @@ __device__ __forceinline__ void trace_one(const SceneDev& sc, const TraceArgs& a
       break;
     }
     Hit h;
-    if (!intersect(sc, org, dir, kRayEps, __int_as_float(0x7f7fffff), h))
+    if (!intersect_t<STACK>(sc, org, dir, kRayEps, __int_as_float(0x7f7fffff), h))
       break;  // photon goes to the sky
     const Surf s = surface_at(sc, org, dir, h);
     const Material& m = sc.mat[h.prim];
@@ -172,14 +173,14 @@ __global__ void __launch_bounds__(128)
     for (int t = threadIdx.x; t < 3 * a.n_params; t += blockDim.x) rs.g[t] = 0.f;
     for (int j = 0; j < a.n_params; ++j) rs.cnt[j][threadIdx.x] = 0;
     __syncthreads();
-    if (i < a.n_emit) trace_one<MODE>(sc, a, i, &rs);
+    if (i < a.n_emit) trace_one<MODE, kBvhStack>(sc, a, i, &rs);
     __syncthreads();
     for (int t = threadIdx.x; t < 3 * a.n_params; t += blockDim.x)
       if (rs.g[t] != 0.f) atomicAdd(a.grad + t, (double)rs.g[t]);
     return;
   }
   if (i >= a.n_emit) return;
-  trace_one<MODE>(sc, a, i, nullptr);
+  trace_one<MODE, kBvhStack>(sc, a, i, nullptr);
 }
 
 __global__ void gather_photons_kernel(const float* __restrict__ raw,
@@ -191,6 +192,41 @@ __global__ void gather_photons_kernel(const float* __restrict__ raw,
   float* o = out + 9 * (size_t)s;
 #pragma unroll
   for (int j = 0; j < 9; ++j) o[j] = r[j];
+}
+
+// Every emitted photon of every scene of a batch, one thread each: the
+// global map rule, appended to the scene's own region.
+template <int STACK>
+__global__ void __launch_bounds__(256)
+    batch_trace_kernel(BatchTables t, int64_t total) {
+  __shared__ int64_t off[kMaxBatchScenes + 1];
+  batch_load_offsets(off, t.emit_off, t.n_scenes);
+  __syncthreads();
+  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (g >= total) return;
+  const int s = batch_find(off, t.n_scenes, g);
+  const BatchScene& bs = t.scenes[s];
+  TraceArgs a{};
+  a.seed = bs.seed;
+  a.n_emit = bs.n_emit;
+  a.max_depth = bs.max_depth;
+  a.caustic = 0;
+  a.out = bs.raw;
+  a.keys = bs.keys;
+  a.counter = bs.counter;
+  a.cap = bs.cap;
+  a.status = t.status;
+  trace_one<kTracePlain, STACK>(bs.sc, a, (int)(g - off[s]), nullptr);
+}
+
+void batch_trace_launch(const BatchTables& t, int64_t total_emit, int block, int stack,
+                        cudaStream_t st) {
+  if (total_emit <= 0) return;
+  const unsigned gb = (unsigned)((total_emit + block - 1) / block);
+  if (stack <= 32)
+    batch_trace_kernel<32><<<gb, block, 0, st>>>(t, total_emit);
+  else
+    batch_trace_kernel<64><<<gb, block, 0, st>>>(t, total_emit);
 }
 
 // first[p] = sorted index of the first stored photon of emitted photon p.

@@ -79,3 +79,18 @@ def test_oracle_intersect_basic():
     r = np.array([[0.5, 0.5, 0.5, 1e-5, 0, -1, 0, 1e30]], np.float32)
     h = sc.intersect(r)
     assert abs(h[0, 0] - 0.5) < 1e-6 and m.names[h[0, 3].view(np.int32)] == "floor"
+
+
+def test_batch_scene_generator():
+    """Scenes of the batched benchmark: triangle count in range (the floor
+    grid plus 1-40 boxes), settings in range, reproducible from the seed."""
+    from photon_mapping_b200 import batch as B
+    for seed in range(4):
+        sc = B.random_scene(seed)
+        assert 450 <= sc["mesh"].n_faces <= 520_000
+        assert 100_000 <= sc["photons"] <= 4_000_000
+        assert 128 <= sc["width"] == sc["height"] <= 1024
+        assert sc["k"] in (50, 100)
+        again = B.random_scene(seed)
+        assert np.array_equal(again["mesh"].vertices, sc["mesh"].vertices)
+        assert sum(1 for nm in sc["mesh"].names if nm == "light") == 2
