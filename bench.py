@@ -92,6 +92,17 @@ def dist_env():
     return world, rank, local
 
 
+def max_over_ranks(dist, value: float, device) -> float:
+    """The largest `value` over all ranks (every rank gets it); the value
+    itself without a process group."""
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_init(world: int, backend: str):
     if world <= 1:
         return None
@@ -472,11 +483,7 @@ def run_ours(args) -> None:
     if dist:
         dist.barrier()
     times = [e0.elapsed_time(e1) for e0, e1 in evs]
-    ms = sum(times) / len(times)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, sum(times) / len(times), dev)
     value = world * nq / (ms / 1e3)
 
     # e2e through the C ABI with pinned host buffers
@@ -499,11 +506,7 @@ def run_ours(args) -> None:
         t0 = time.perf_counter()
         e2e_step()
         e2e_times.append(time.perf_counter() - t0)
-    e2e_s = sum(e2e_times) / len(e2e_times)
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(dist, sum(e2e_times) / len(e2e_times), dev)
     e2e_value = world * nq / e2e_s
     clk = clocks.stop()  # sampled over the timed steps and the e2e steps
 

@@ -78,6 +78,39 @@ class Image:
     def gammaCorrection(self, gamma: float):  # image.h:58-67
         self.pixels = np.power(self.pixels, F(1.0) / F(gamma)).astype(F)
 
+    def writePFM(self, filename: str):
+        """Raw linear radiance as a little-endian colour PFM ("PF", scale
+        -1), rows stored bottom to top as the format defines. The reference
+        writes only clamped 8-bit PPM (image.h:69-90); PFM keeps the float
+        values for comparisons such as the image error against the path
+        tracer."""
+        with open(filename, "wb") as f:
+            f.write(f"PF\n{self.width} {self.height}\n-1.0\n".encode("ascii"))
+            f.write(np.ascontiguousarray(self.pixels[::-1], dtype="<f4").tobytes())
+
+    @classmethod
+    def readPFM(cls, filename: str) -> "Image":
+        """Reads a colour PFM written by writePFM (or any little- or
+        big-endian "PF" file)."""
+        with open(filename, "rb") as f:
+            data = f.read()
+        parts, pos = [], 0
+        while len(parts) < 4:  # "PF", width, height, scale (whitespace separated)
+            while data[pos:pos + 1].isspace():
+                pos += 1
+            end = pos
+            while not data[end:end + 1].isspace():
+                end += 1
+            parts.append(data[pos:end].decode("ascii"))
+            pos = end
+        pos += 1  # the single whitespace byte after the scale
+        if parts[0] != "PF":
+            raise ValueError(f"{filename}: not a colour PFM file")
+        w, h, scale = int(parts[1]), int(parts[2]), float(parts[3])
+        dt = "<f4" if scale < 0 else ">f4"
+        px = np.frombuffer(data, dtype=dt, count=w * h * 3, offset=pos).reshape(h, w, 3)
+        return cls(w, h, px[::-1].astype(F))
+
     def writePPM(self, filename: str):  # image.h:69-90 (P3, clamped to 0..255)
         v = (F(255.0) * self.pixels)
         with np.errstate(invalid="ignore"):

@@ -34,6 +34,38 @@ def radiance_queries(pos, wo, ns, rho) -> np.ndarray:
     return q
 
 
+# Binary photon file: 16-byte header {magic "PMPH", version 1 (u32), photon
+# count (u64)}, the number of photons emitted (u64), then count records of 9
+# little-endian float32 {throughput, position, wi} (photon_map.h:10-22).
+PHOTON_FILE_MAGIC = b"PMPH"
+
+
+def save_photons(path, photons, n_emitted: int) -> None:
+    """Writes a photon set and the number of photons emitted to make it
+    (the estimate's normalisation, integrator.h:149)."""
+    a = np.ascontiguousarray(as_photons(photons), dtype="<f4")
+    with open(path, "wb") as f:
+        f.write(PHOTON_FILE_MAGIC + np.array([1], "<u4").tobytes() +
+                np.array([a.shape[0], int(n_emitted)], "<u8").tobytes())
+        f.write(a.tobytes())
+
+
+def load_photons(path) -> tuple[np.ndarray, int]:
+    """Reads a file of save_photons: (photons (n, 9) float32, n_emitted)."""
+    with open(path, "rb") as f:
+        head = f.read(24)
+        if len(head) != 24 or head[:4] != PHOTON_FILE_MAGIC:
+            raise ValueError(f"{path}: not a photon file")
+        version = int(np.frombuffer(head, "<u4", 1, 4)[0])
+        if version != 1:
+            raise ValueError(f"{path}: photon file version {version}")
+        n, emitted = (int(x) for x in np.frombuffer(head, "<u8", 2, 8))
+        body = f.read()
+    if len(body) != n * 36:
+        raise ValueError(f"{path}: {len(body)} bytes for {n} photons")
+    return np.frombuffer(body, "<f4").reshape(n, 9).astype(np.float32), emitted
+
+
 class PhotonMap:
     """A photon map living on the device (one of the context's two maps)."""
 
@@ -89,6 +121,21 @@ class PhotonMap:
                            "pm_photonmap_get_photons")
         return out
 
+    def save(self, path, n_emitted: int) -> None:
+        """Writes the map's photons (index order) to a photon file."""
+        save_photons(path, self.photons(), n_emitted)
+
+    def load(self, path) -> int:
+        """Replaces the photons with a photon file's and builds the map;
+        returns the number of photons emitted recorded in the file."""
+        photons, emitted = load_photons(path)
+        self.setPhotons(photons)
+        self.build()
+        self.ctx.check(self.ctx.lib.pm_photonmap_set_emitted(self.ctx.handle, self.map_id,
+                                                             int(emitted)),
+                       "pm_photonmap_set_emitted")
+        return emitted
+
     # photon_map.h:208-211
     def queryKNearestPhotons(self, p, k: int) -> tuple[list[int], float]:
         idx, cnt, md2 = self.query_knn(np.asarray(p, dtype=np.float32).reshape(1, 3), k)
@@ -117,4 +164,5 @@ class PhotonMap:
         return out
 
 
-__all__ = ["PhotonMap", "PMError", "radiance_queries", "as_photons"]
+__all__ = ["PhotonMap", "PMError", "radiance_queries", "as_photons", "save_photons",
+           "load_photons"]
