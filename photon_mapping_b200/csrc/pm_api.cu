@@ -2,6 +2,7 @@
 // declared in include/pm_cuda.h.
 #include "../../include/pm_cuda.h"
 #include "pm_api_internal.cuh"
+#include "pm_hostio.cuh"
 
 #include <cstdio>
 #include <cstring>
@@ -320,22 +321,23 @@ int pm_photonmap_knn(pm_ctx* c, int map, const float* queries, int64_t nq,
   if ((s = c->q_in.ensure(qb)) || (s = c->q_out.ensure(ib + cb + mb)))
     return set_err(c, s, "query buffers");
   cudaStream_t st = c->stream;
-  cudaError_t e =
-      cudaMemcpyAsync(c->q_in.ptr, queries, qb, cudaMemcpyHostToDevice, st);
+  cudaError_t e = copy_in(c->q_in.ptr, queries, qb, c->num_sms, st);
   if (e != cudaSuccess) return cuda_status(c, e, "query upload");
+  // mapped output buffers are written by the kernel itself
+  int32_t* m_idx = (int32_t*)mapped_host(out_idx);
+  int32_t* m_cnt = (int32_t*)mapped_host(out_count);
+  float* m_md2 = (float*)mapped_host(out_maxdist2);
   KnnOut o{};
   o.stats = c->stats_ptr();
-  o.idx = (int32_t*)c->q_out.ptr;
-  o.count = (int32_t*)((char*)c->q_out.ptr + ib);
-  o.maxd2 = (float*)((char*)c->q_out.ptr + ib + cb);
+  o.idx = m_idx ? m_idx : (int32_t*)c->q_out.ptr;
+  o.count = m_cnt ? m_cnt : (int32_t*)((char*)c->q_out.ptr + ib);
+  o.maxd2 = m_md2 ? m_md2 : (float*)((char*)c->q_out.ptr + ib + cb);
   e = knn_launch(map_view(dm), c->q_in.ptr, nq, k, kModeKnn, 0.f, o,
                  c->next_counter(), c->num_sms, st);
   if (e != cudaSuccess) return cuda_status(c, e, "knn launch");
-  if ((e = cudaMemcpyAsync(out_idx, o.idx, ib, cudaMemcpyDeviceToHost, st)) ||
-      (e = cudaMemcpyAsync(out_count, o.count, cb, cudaMemcpyDeviceToHost,
-                           st)) ||
-      (e = cudaMemcpyAsync(out_maxdist2, o.maxd2, mb, cudaMemcpyDeviceToHost,
-                           st)))
+  if ((!m_idx && (e = cudaMemcpyAsync(out_idx, o.idx, ib, cudaMemcpyDeviceToHost, st))) ||
+      (!m_cnt && (e = cudaMemcpyAsync(out_count, o.count, cb, cudaMemcpyDeviceToHost, st))) ||
+      (!m_md2 && (e = cudaMemcpyAsync(out_maxdist2, o.maxd2, mb, cudaMemcpyDeviceToHost, st))))
     return cuda_status(c, e, "knn download");
   return cuda_status(c, cudaStreamSynchronize(st), "knn");
 }
@@ -361,17 +363,20 @@ int pm_photonmap_radiance(pm_ctx* c, int map, const pm_radiance_query* q,
   if ((s = c->q_in.ensure(qb)) || (s = c->q_out.ensure(ob)))
     return set_err(c, s, "query buffers");
   cudaStream_t st = c->stream;
-  cudaError_t e = cudaMemcpyAsync(c->q_in.ptr, q, qb, cudaMemcpyHostToDevice,
-                                  st);
+  cudaError_t e = copy_in(c->q_in.ptr, q, qb, c->num_sms, st);
   if (e != cudaSuccess) return cuda_status(c, e, "query upload");
+  // a mapped output buffer is written by the kernel itself
+  float* mapped_out = (float*)mapped_host(out_rgb);
   KnnOut o{};
   o.stats = c->stats_ptr();
-  o.rgb = (float*)c->q_out.ptr;
+  o.rgb = mapped_out ? mapped_out : (float*)c->q_out.ptr;
   e = knn_launch(map_view(dm), c->q_in.ptr, nq, k, kModeRadiance,
                  (float)n_emitted, o, c->next_counter(), c->num_sms, st);
   if (e != cudaSuccess) return cuda_status(c, e, "radiance launch");
-  e = cudaMemcpyAsync(out_rgb, o.rgb, ob, cudaMemcpyDeviceToHost, st);
-  if (e != cudaSuccess) return cuda_status(c, e, "radiance download");
+  if (!mapped_out) {
+    e = cudaMemcpyAsync(out_rgb, o.rgb, ob, cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) return cuda_status(c, e, "radiance download");
+  }
   return cuda_status(c, cudaStreamSynchronize(st), "radiance");
 }
 

@@ -1050,7 +1050,7 @@ template <int C>
 __global__ void __launch_bounds__(256, 4)
     knn_batch_kernel(BatchTables t, const float4* __restrict__ slots,
                      const uint32_t* __restrict__ order, const int64_t* __restrict__ qoff,
-                     const int64_t* __restrict__ item_off, int chunk, float* __restrict__ res,
+                     const int64_t* __restrict__ item_off, int chunk, KnnOut out,
                      unsigned long long* __restrict__ counter) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int64_t ioff[kMaxBatchScenes + 1];
@@ -1064,8 +1064,6 @@ __global__ void __launch_bounds__(256, 4)
   float r_hint = -1.f;
   int cur = -1, k = 0;
   float n_emitted = 0.f;
-  KnnOut out{};
-  out.rgb = res;
   while (true) {
     unsigned long long c0 = 0;
     if (lane == 0) c0 = atomicAdd(counter, 1ull);
@@ -1124,7 +1122,9 @@ cudaError_t batch_knn_launch(const BatchTables& t, const float4* slots, const ui
   if (blocks < 1) blocks = 1;
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
-  kern<<<(unsigned)blocks, threads, smem, st>>>(t, slots, order, qoff, item_off, chunk, res,
+  KnnOut out{};
+  out.rgb = res;
+  kern<<<(unsigned)blocks, threads, smem, st>>>(t, slots, order, qoff, item_off, chunk, out,
                                                 counter);
   return cudaGetLastError();
 }

@@ -174,3 +174,37 @@ def test_large_map_properties(ctx):
     rad = pm.radiance(q, 100, n)
     assert_radiance_close(rad[sample], O.radiance_fp64(ph, oidx, ocnt, omd2, q[sample], n),
                           what="1M sample")
+
+
+def test_page_locked_host_buffers(ctx):
+    """Host-pointer calls with page-locked (mapped) buffers fetch the
+    queries with a copy kernel and write the results straight into the
+    host buffers; the results equal those of pageable buffers."""
+    import ctypes as C
+    import torch
+    ph = W.wall_photons(100000, seed=7)
+    pm = gpu_map(ctx, ph)
+    q = W.wall_queries(70001, seed=8)
+    want = pm.radiance(q, 50, 100000)
+    widx, wcnt, wmd2 = pm.query_knn(q[:, :3], 30)
+    hq = torch.from_numpy(np.ascontiguousarray(q)).pin_memory()
+    hout = torch.zeros((q.shape[0], 3), dtype=torch.float32).pin_memory()
+    ctx.check(ctx.lib.pm_photonmap_radiance(ctx.handle, 0, hq.data_ptr(), q.shape[0], 50, 100000,
+                                            hout.data_ptr()), "pm_photonmap_radiance")
+    np.testing.assert_array_equal(hout.numpy(), want)
+    hp = torch.from_numpy(np.ascontiguousarray(q[:, :3])).pin_memory()
+    hidx = torch.zeros((q.shape[0], 30), dtype=torch.int32).pin_memory()
+    hcnt = torch.zeros(q.shape[0], dtype=torch.int32).pin_memory()
+    hmd2 = torch.zeros(q.shape[0], dtype=torch.float32).pin_memory()
+    ctx.check(ctx.lib.pm_photonmap_knn(ctx.handle, 0, hp.data_ptr(), q.shape[0], 30,
+                                       hidx.data_ptr(), hcnt.data_ptr(), hmd2.data_ptr()),
+              "pm_photonmap_knn")
+    np.testing.assert_array_equal(hidx.numpy(), widx)
+    np.testing.assert_array_equal(hcnt.numpy(), wcnt)
+    np.testing.assert_array_equal(hmd2.numpy(), wmd2)
+    # a query array whose size is not a multiple of 16 bytes (3 floats each)
+    hp1 = torch.from_numpy(np.ascontiguousarray(q[:5, :3])).pin_memory()
+    i1, c1, m1 = (np.zeros((5, 30), np.int32), np.zeros(5, np.int32), np.zeros(5, np.float32))
+    ctx.check(ctx.lib.pm_photonmap_knn(ctx.handle, 0, hp1.data_ptr(), 5, 30, i1.ctypes.data,
+                                       c1.ctypes.data, m1.ctypes.data), "pm_photonmap_knn")
+    np.testing.assert_array_equal(i1, widx[:5])
