@@ -147,13 +147,16 @@ int upload_tables(pm_batch* b) {
     x.qinv = make_float3(sc.hi[0] > sc.lo[0] ? 1.0f / (sc.hi[0] - sc.lo[0]) : 0.f,
                          sc.hi[1] > sc.lo[1] ? 1.0f / (sc.hi[1] - sc.lo[1]) : 0.f,
                          sc.hi[2] > sc.lo[2] ? 1.0f / (sc.hi[2] - sc.lo[2]) : 0.f);
-    x.seed = d.seed;
-    x.n_emit = (int)d.n_photons;
-    x.max_depth = d.max_depth;
-    x.raw = (float*)b->raw.ptr + 9 * b->cap_off[s];
-    x.keys = (unsigned long long*)b->keys.ptr + b->cap_off[s];
-    x.counter = (unsigned long long*)b->counters.ptr + s;
-    x.cap = (unsigned long long)b->cap[s];
+    TraceArgs& ta = x.ta;
+    ta.seed = d.seed;
+    ta.n_emit = (int)d.n_photons;
+    ta.max_depth = d.max_depth;
+    ta.caustic = 0;
+    ta.out = (float*)b->raw.ptr + 9 * b->cap_off[s];
+    ta.keys = (unsigned long long*)b->keys.ptr + b->cap_off[s];
+    ta.counter = (unsigned long long*)b->counters.ptr + s;
+    ta.cap = (unsigned long long)b->cap[s];
+    ta.status = (unsigned*)b->status.ptr;
     x.res = (float*)b->res.ptr + 3 * b->slot_off[s];
     x.accum = nullptr;
     x.image = (float*)b->images.ptr + 3 * b->pix_off[s];
@@ -181,6 +184,7 @@ int upload_tables(pm_batch* b) {
   bt.slots = (const float4*)b->slots.ptr;
   bt.n_scenes = n;
   bt.status = (unsigned*)b->status.ptr;
+  bt.next_photon = (unsigned long long*)((char*)b->status.ptr + 16);
   bt.dropped = (unsigned long long*)b->dropped.ptr;
   return PM_OK;
 }

@@ -297,6 +297,7 @@ extern "C" int pm_diff_backward(pm_ctx* c, const float* grad_rgb, float* grad_al
     t.max_depth = d.max_depth;
     t.caustic = map;
     t.cap = (unsigned long long)c->maps[map].n;
+    t.next = (unsigned long long*)((char*)c->trace_misc.ptr + 32);
     t.dmat = (const Material*)d.dec_mat.ptr;
     t.first = (const uint32_t*)d.first[map].ptr;
     t.adj = padj[map];

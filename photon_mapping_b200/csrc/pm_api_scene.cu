@@ -144,6 +144,7 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
     a.counter = counter;
     a.cap = cap;
     a.status = status;
+    a.next = (unsigned long long*)((char*)c->trace_misc.ptr + 32);
     a.dmat = dmat;
     trace_launch(c->scene_view(), a, st);
     if ((e = cudaGetLastError()) != cudaSuccess)

@@ -21,13 +21,7 @@ struct BatchScene {
   int k;               // nEstimationGlobal
   float n_emitted;     // photons emitted for the map
   float3 qlo, qinv;    // box of the query Morton codes (vertex bounds)
-  // photon trace: this scene's append region
-  unsigned long long seed;
-  int n_emit, max_depth;
-  float* raw;
-  unsigned long long* keys;
-  unsigned long long* counter;
-  unsigned long long cap;
+  TraceArgs ta;         // photon trace into this scene's append region
   // resolve
   float* res;          // the estimates of this scene's slots
   float4* accum;
@@ -60,6 +54,7 @@ struct BatchTables {
   const float4* slots;       // the query slots of all scenes (4 float4 each)
   int n_scenes;
   unsigned* status;             // trace NaN / negative stops (2 words)
+  unsigned long long* next_photon;  // work counter of the batched trace
   unsigned long long* dropped;  // NaN / negative samples (2 words)
 };
 

@@ -18,6 +18,8 @@
 #include "pm_sort.cuh"
 #include "pm_trace.cuh"
 
+#include <algorithm>
+
 namespace pm {
 
 __host__ __device__ __forceinline__ unsigned long long splitmix64(
@@ -54,133 +56,194 @@ struct ReplaySmem {
   unsigned char cnt[kMaxDiffParams][128];
 };
 
-// One emitted photon of PhotonMapping::build (integrator.h:406-469 global,
-// :483-558 caustics).
-template <int MODE, int STACK>
-__device__ __forceinline__ void trace_one(const SceneDev& sc, const TraceArgs& a, int i,
-                                          ReplaySmem* rs) {
-  Rng rng{photon_stream_state(a.seed, (unsigned long long)i)};
+// State of one photon path between bounces.
+struct PhotonPath {
+  Rng rng;
+  V3 thr, td;     // throughput, and the decision throughput (frozen mode)
+  V3 org, dir;
+  int i;          // photon index within its map
+  int k;          // bounce
+  int nst;        // photons stored so far (replay)
+  bool prev_specular;
+};
 
-  // sampleRayFromLight (integrator.h:265-288)
+// sampleRayFromLight (integrator.h:265-288): the start of photon i.
+template <int MODE>
+__device__ __forceinline__ void photon_emit(const SceneDev& sc, const TraceArgs& a, int i,
+                                            PhotonPath& p) {
+  p.rng = Rng{photon_stream_state(a.seed, (unsigned long long)i)};
   float pdf_choose, pdf_pos, pdf_dir;
-  const int lf = sample_light(sc, rng, pdf_choose);
-  const Surf ls = sample_triangle(sc, lf, rng, pdf_pos);
+  const int lf = sample_light(sc, p.rng, pdf_choose);
+  const Surf ls = sample_triangle(sc, lf, p.rng, pdf_pos);
   float u0, u1;
-  rng.next2d(u0, u1);
+  p.rng.next2d(u0, u1);
   const V3 dl = sample_cos_hemisphere(u0, u1, pdf_dir);
-  V3 dir = local_to_world(dl, ls.dpdu, ls.ns, ls.dpdv);
+  p.dir = local_to_world(dl, ls.dpdu, ls.ns, ls.dpdv);
   const Material& lm = sc.mat[lf];
-  V3 thr = v3(lm.le[0], lm.le[1], lm.le[2]) /
-           (pdf_choose * pdf_pos * pdf_dir) * fabsf(dot(dir, ls.ns));
+  p.thr = v3(lm.le[0], lm.le[1], lm.le[2]) /
+          (pdf_choose * pdf_pos * pdf_dir) * fabsf(dot(p.dir, ls.ns));
   // decision throughput: the same arithmetic over the decision materials
-  V3 td = thr;
+  p.td = p.thr;
   if (MODE != kTracePlain) {
     const Material& dm = a.dmat[lf];
-    td = v3(dm.le[0], dm.le[1], dm.le[2]) /
-         (pdf_choose * pdf_pos * pdf_dir) * fabsf(dot(dir, ls.ns));
+    p.td = v3(dm.le[0], dm.le[1], dm.le[2]) /
+           (pdf_choose * pdf_pos * pdf_dir) * fabsf(dot(p.dir, ls.ns));
   }
-  V3 org = ls.pos;
-  int nst = 0;  // replay: photons this path has stored so far
+  p.org = ls.pos;
+  p.i = i;
+  p.k = 0;
+  p.nst = 0;
+  p.prev_specular = false;
+}
 
-  bool prev_specular = false;
-  for (int k = 0; k < a.max_depth; ++k) {
-    const V3 dec = MODE != kTracePlain ? td : thr;
-    if (has_nan(dec)) {
-      if (MODE != kTraceReplay) atomicAdd(a.status + 0, 1u);
-      break;
-    }
-    if (dec.x < 0.f || dec.y < 0.f || dec.z < 0.f) {
-      if (MODE != kTraceReplay) atomicAdd(a.status + 1, 1u);
-      break;
-    }
-    Hit h;
-    if (!intersect_t<STACK>(sc, org, dir, kRayEps, __int_as_float(0x7f7fffff), h))
-      break;  // photon goes to the sky
-    const Surf s = surface_at(sc, org, dir, h);
-    const Material& m = sc.mat[h.prim];
-    const bool diffuse = m.type == kLambert;
-    bool store = false, stop = false;
-    if (!a.caustic) {
-      store = diffuse;
-    } else {
-      // integrator.h:510-523
-      if (!prev_specular && diffuse) break;
-      if (prev_specular && diffuse) store = stop = true;
-      prev_specular = !diffuse;
-    }
-    if (store) {
-      if (MODE == kTraceReplay) {
-        // the replay stores where the trace stored; cap = photons stored
-        const unsigned long long si = (unsigned long long)a.first[i] + (unsigned)nst;
-        if (si >= a.cap) {
-          atomicOr(sc.err, 8);
-          break;
-        }
-        const float4 g = a.adj[si];
-        const V3 w = v3(g.x, g.y, g.z) * thr;
-        for (int j = 0; j < a.n_params; ++j) {
-          const unsigned c = rs->cnt[j][threadIdx.x];
-          if (c) {
-            atomicAdd(&rs->g[3 * j + 0], (float)c * w.x);
-            atomicAdd(&rs->g[3 * j + 1], (float)c * w.y);
-            atomicAdd(&rs->g[3 * j + 2], (float)c * w.z);
-          }
-        }
-      } else {
-        store_photon(a, i, k, thr, s.pos, -dir);
-      }
-      ++nst;
-    }
-    if (stop) break;
-    // Russian roulette (integrator.h:441-449)
-    if (k > 0) {
-      const float q =
-          fminf(fmaxf(dec.x, fmaxf(dec.y, dec.z)), 1.0f);
-      if (rng.next1d() >= q) break;
-      thr = thr / q;
-      if (MODE != kTracePlain) td = td / q;
-    }
-    // Primitive::sampleBxDF FROM_LIGHT (primitive.h:46-62)
-    const V3 wo = -dir;
-    const V3 wo_l = world_to_local(wo, s.dpdu, s.ns, s.dpdv);
-    V3 wi_l;
-    float pdf;
-    const V3 f = bxdf_sample(m, wo_l, kFromLight, rng, wi_l, pdf);
-    const V3 wi = local_to_world(wi_l, s.dpdu, s.ns, s.dpdv);
-    const float ct = cos_term(wo, wi, s.ns, s.ng, kFromLight);
-    thr = thr * (f * ct / pdf);
-    if (MODE != kTracePlain) {
-      // albedo parameters sit on Lambert faces only; the direction drawn
-      // does not depend on the albedo
-      const V3 fd = diffuse ? lambert_eval(a.dmat[h.prim], wo_l, wi_l) : f;
-      td = td * (fd * ct / pdf);
-    }
+// One iteration k of the tracing loop (integrator.h:417-468 global,
+// :497-557 caustics); false when the path ends.
+template <int MODE, int STACK>
+__device__ __forceinline__ bool photon_step(const SceneDev& sc, const TraceArgs& a,
+                                            PhotonPath& p, ReplaySmem* rs) {
+  if (p.k >= a.max_depth) return false;
+  const V3 dec = MODE != kTracePlain ? p.td : p.thr;
+  if (has_nan(dec)) {
+    if (MODE != kTraceReplay) atomicAdd(a.status + 0, 1u);
+    return false;
+  }
+  if (dec.x < 0.f || dec.y < 0.f || dec.z < 0.f) {
+    if (MODE != kTraceReplay) atomicAdd(a.status + 1, 1u);
+    return false;
+  }
+  Hit h;
+  if (!intersect_t<STACK>(sc, p.org, p.dir, kRayEps, __int_as_float(0x7f7fffff), h))
+    return false;  // photon goes to the sky
+  const Surf s = surface_at(sc, p.org, p.dir, h);
+  const Material& m = sc.mat[h.prim];
+  const bool diffuse = m.type == kLambert;
+  bool store = false, stop = false;
+  if (!a.caustic) {
+    store = diffuse;
+  } else {
+    // integrator.h:510-523
+    if (!p.prev_specular && diffuse) return false;
+    if (p.prev_specular && diffuse) store = stop = true;
+    p.prev_specular = !diffuse;
+  }
+  if (store) {
     if (MODE == kTraceReplay) {
-      const int pid = a.face_pid[h.prim];
-      if (pid >= 0) ++rs->cnt[pid][threadIdx.x];
+      // the replay stores where the trace stored; cap = photons stored
+      const unsigned long long si = (unsigned long long)a.first[p.i] + (unsigned)p.nst;
+      if (si >= a.cap) {
+        atomicOr(sc.err, 8);
+        return false;
+      }
+      const float4 g = a.adj[si];
+      const V3 w = v3(g.x, g.y, g.z) * p.thr;
+      for (int j = 0; j < a.n_params; ++j) {
+        const unsigned c = rs->cnt[j][threadIdx.x];
+        if (c) {
+          atomicAdd(&rs->g[3 * j + 0], (float)c * w.x);
+          atomicAdd(&rs->g[3 * j + 1], (float)c * w.y);
+          atomicAdd(&rs->g[3 * j + 2], (float)c * w.z);
+        }
+      }
+    } else {
+      store_photon(a, p.i, p.k, p.thr, s.pos, -p.dir);
     }
-    org = s.pos;
-    dir = wi;
+    ++p.nst;
+  }
+  if (stop) return false;
+  // Russian roulette (integrator.h:441-449)
+  if (p.k > 0) {
+    const float q = fminf(fmaxf(dec.x, fmaxf(dec.y, dec.z)), 1.0f);
+    if (p.rng.next1d() >= q) return false;
+    p.thr = p.thr / q;
+    if (MODE != kTracePlain) p.td = p.td / q;
+  }
+  // Primitive::sampleBxDF FROM_LIGHT (primitive.h:46-62)
+  const V3 wo = -p.dir;
+  const V3 wo_l = world_to_local(wo, s.dpdu, s.ns, s.dpdv);
+  V3 wi_l;
+  float pdf;
+  const V3 f = bxdf_sample(m, wo_l, kFromLight, p.rng, wi_l, pdf);
+  const V3 wi = local_to_world(wi_l, s.dpdu, s.ns, s.dpdv);
+  const float ct = cos_term(wo, wi, s.ns, s.ng, kFromLight);
+  p.thr = p.thr * (f * ct / pdf);
+  if (MODE != kTracePlain) {
+    // albedo parameters sit on Lambert faces only; the direction drawn
+    // does not depend on the albedo
+    const V3 fd = diffuse ? lambert_eval(a.dmat[h.prim], wo_l, wi_l) : f;
+    p.td = p.td * (fd * ct / pdf);
+  }
+  if (MODE == kTraceReplay) {
+    const int pid = a.face_pid[h.prim];
+    if (pid >= 0) ++rs->cnt[pid][threadIdx.x];
+  }
+  p.org = s.pos;
+  p.dir = wi;
+  ++p.k;
+  return true;
+}
+
+// Persistent tracing with regeneration: paths end after very different
+// numbers of bounces (Russian roulette, escapes), so instead of one photon
+// per thread, a thread whose path ended takes the next photon index (one
+// atomic per warp for all its lanes that need one) and the warp keeps its
+// lanes busy until the indices run out. The photons traced, and what they
+// store, do not depend on which thread traces them.
+// scene(src) and args(src) give the scene and trace arguments of source src
+// (a scene of a batch, or the kernel's only one); first(g, src) maps the
+// work index g to (source, photon index).
+template <int MODE, int STACK, class Scene, class Args, class First>
+__device__ __forceinline__ void trace_persistent(unsigned long long* next, long long total,
+                                                 ReplaySmem* rs, Scene&& scene, Args&& args,
+                                                 First&& first) {
+  const int lane = (int)(threadIdx.x & 31);
+  PhotonPath p;
+  int src = 0;
+  bool live = false, done = false;
+  while (true) {
+    const unsigned want = __ballot_sync(kFull, !live && !done);
+    if (want) {
+      unsigned long long base = 0;
+      const int leader = __ffs(want) - 1;
+      if (lane == leader) base = atomicAdd(next, (unsigned long long)__popc(want));
+      base = __shfl_sync(kFull, base, leader);
+      if (!live && !done) {
+        const unsigned long long g = base + (unsigned)__popc(want & lanemask_lt());
+        if ((long long)g < total) {
+          const int i = first((long long)g, src);
+          photon_emit<MODE>(scene(src), args(src), i, p);
+          if (MODE == kTraceReplay)
+            for (int j = 0; j < args(src).n_params; ++j) rs->cnt[j][threadIdx.x] = 0;
+          live = true;
+        } else {
+          done = true;
+        }
+      }
+    }
+    if (__ballot_sync(kFull, live) == 0) break;
+    if (live) live = photon_step<MODE, STACK>(scene(src), args(src), p, rs);
   }
 }
 
 template <int MODE>
 __global__ void __launch_bounds__(128)
     trace_kernel(SceneDev sc, TraceArgs a) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  auto scene = [&](int) -> const SceneDev& { return sc; };
+  auto args = [&](int) -> const TraceArgs& { return a; };
+  auto first = [](long long g, int& src) {
+    src = 0;
+    return (int)g;
+  };
   if (MODE == kTraceReplay) {
     __shared__ ReplaySmem rs;
     for (int t = threadIdx.x; t < 3 * a.n_params; t += blockDim.x) rs.g[t] = 0.f;
-    for (int j = 0; j < a.n_params; ++j) rs.cnt[j][threadIdx.x] = 0;
     __syncthreads();
-    if (i < a.n_emit) trace_one<MODE, kBvhStack>(sc, a, i, &rs);
+    trace_persistent<MODE, kBvhStack>(a.next, a.n_emit, &rs, scene, args, first);
     __syncthreads();
     for (int t = threadIdx.x; t < 3 * a.n_params; t += blockDim.x)
       if (rs.g[t] != 0.f) atomicAdd(a.grad + t, (double)rs.g[t]);
     return;
   }
-  if (i >= a.n_emit) return;
-  trace_one<MODE, kBvhStack>(sc, a, i, nullptr);
+  trace_persistent<MODE, kBvhStack>(a.next, a.n_emit, nullptr, scene, args, first);
 }
 
 __global__ void gather_photons_kernel(const float* __restrict__ raw,
@@ -194,35 +257,38 @@ __global__ void gather_photons_kernel(const float* __restrict__ raw,
   for (int j = 0; j < 9; ++j) o[j] = r[j];
 }
 
-// Every emitted photon of every scene of a batch, one thread each: the
-// global map rule, appended to the scene's own region.
+// Every emitted photon of every scene of a batch: the global map rule, each
+// scene appending to its own region. Persistent: the photon index runs over
+// all scenes' photons, the scene found by binary search.
 template <int STACK>
 __global__ void __launch_bounds__(256)
     batch_trace_kernel(BatchTables t, int64_t total) {
   __shared__ int64_t off[kMaxBatchScenes + 1];
   batch_load_offsets(off, t.emit_off, t.n_scenes);
   __syncthreads();
-  const int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (g >= total) return;
-  const int s = batch_find(off, t.n_scenes, g);
-  const BatchScene& bs = t.scenes[s];
-  TraceArgs a{};
-  a.seed = bs.seed;
-  a.n_emit = bs.n_emit;
-  a.max_depth = bs.max_depth;
-  a.caustic = 0;
-  a.out = bs.raw;
-  a.keys = bs.keys;
-  a.counter = bs.counter;
-  a.cap = bs.cap;
-  a.status = t.status;
-  trace_one<kTracePlain, STACK>(bs.sc, a, (int)(g - off[s]), nullptr);
+  auto scene = [&](int s) -> const SceneDev& { return t.scenes[s].sc; };
+  auto args = [&](int s) -> const TraceArgs& { return t.scenes[s].ta; };
+  auto first = [&](long long g, int& src) {
+    src = batch_find(off, t.n_scenes, g);
+    return (int)(g - off[src]);
+  };
+  trace_persistent<kTracePlain, STACK>(t.next_photon, total, nullptr, scene, args, first);
+}
+
+static int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
 }
 
 void batch_trace_launch(const BatchTables& t, int64_t total_emit, int block, int stack,
                         cudaStream_t st) {
   if (total_emit <= 0) return;
-  const unsigned gb = (unsigned)((total_emit + block - 1) / block);
+  // persistent: as many blocks as fit at once (2048 threads per SM)
+  const long long cap = (long long)sm_count() * (2048 / block);
+  const unsigned gb = (unsigned)std::min<long long>(cap, (total_emit + block - 1) / block);
+  cudaMemsetAsync(t.next_photon, 0, sizeof(unsigned long long), st);
   if (stack <= 32)
     batch_trace_kernel<32><<<gb, block, 0, st>>>(t, total_emit);
   else
@@ -246,7 +312,10 @@ __global__ void iota_kernel(uint32_t* v, int n) {
 void trace_launch(const SceneDev& sc, const TraceArgs& a, cudaStream_t st) {
   if (a.n_emit <= 0) return;
   const int tb = 128;  // ReplaySmem holds 128 threads' counters
-  const int gb = (a.n_emit + tb - 1) / tb;
+  // persistent: as many blocks as fit at once (2048 threads per SM)
+  const long long cap = (long long)sm_count() * (2048 / tb);
+  const int gb = (int)std::min<long long>(cap, (a.n_emit + tb - 1) / tb);
+  cudaMemsetAsync(a.next, 0, sizeof(unsigned long long), st);
   if (a.adj)
     trace_kernel<kTraceReplay><<<gb, tb, 0, st>>>(sc, a);
   else if (a.dmat)
