@@ -223,6 +223,11 @@ RENDER_CONFIGS = {
     # (integrator.h:292-309), the setting its CPU time is taken on
     "config2_gather1": dict(width=512, height=512, spp=4, photons=1_000_000, k=100, fg=1,
                             n_gather=1),
+    # caustics scene (mirror and glass icospheres, 512x512 water
+    # heightfield; 563,238 triangles), 1M global + 10M caustics photons,
+    # k=100, final gathering; timed on 2 of its 64 spp
+    "config3": dict(width=512, height=512, spp=2, photons=1_000_000, k=100, fg=1, n_gather=1,
+                    scene="caustics", caustics_multiplier=10.0),
 }
 CPU_RENDER_BUDGET_S = 6.0   # per config, for the reference integrator's bounded sample
 
@@ -263,11 +268,25 @@ def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
     the configs above, photon maps traced beforehand; beside each, the
     reference integrator's CPU rate where its settings match."""
     import torch
+    from photon_mapping_b200 import scene as S
     from photon_mapping_b200.integrator import PhotonMapping
     out = {}
     for name, c in RENDER_CONFIGS.items():
-        pmi = PhotonMapping(c["photons"], c["k"], 1.0, c["k"], c["fg"], MAX_DEPTH, ctx=ctx)
-        pmi.build(sc, seed=TRACE_SEED)
+        mult = c.get("caustics_multiplier", 1.0)
+        scene_mesh, scene_dev = mesh, sc
+        trace_s = None
+        if c.get("scene") == "caustics":
+            scene_mesh = S.caustics_scene(0)
+            scene_dev = S.Scene(ctx)
+            scene_dev.setMesh(scene_mesh)
+            scene_dev.build()
+        pmi = PhotonMapping(c["photons"], c["k"], mult, c["k"], c["fg"], MAX_DEPTH, ctx=ctx)
+        pmi.build(scene_dev, seed=TRACE_SEED)
+        if c.get("scene") == "caustics":
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            trace = pmi.build(scene_dev, seed=TRACE_SEED)
+            trace_s = time.perf_counter() - t0
         pmi.render(camera, c["width"], c["height"], 1, n_gather=c["n_gather"])  # warm-up
         torch.cuda.synchronize(dev)
         t0 = time.perf_counter()
@@ -275,10 +294,19 @@ def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
         dt = time.perf_counter() - t0
         n = c["width"] * c["height"] * c["spp"]
         out[name] = {"samples_per_s": n / dt, "seconds": dt, **c,
-                     "queries_global": st["queries_global"], "passes": st["passes"],
+                     "queries_global": st["queries_global"],
+                     "queries_caustics": st["queries_caustics"], "passes": st["passes"],
                      "mean_radiance": float(img.mean())}
-        if cpu:
+        if trace_s is not None:
+            out[name]["photon_trace"] = {
+                "seconds": trace_s, "triangles": int(scene_mesh.n_faces),
+                "emitted": c["photons"] + int(c["photons"] * mult),
+                "stored": {k: int(v["stored"]) for k, v in trace.items()},
+                "photons_per_s": (c["photons"] + c["photons"] * mult) / trace_s}
+        if cpu and c.get("scene") != "caustics":
             out[name]["cpu_reference"] = cpu_render_rate(mesh, pmi, c)
+        if scene_dev is not sc:
+            sc.build()   # the bench scene back on the context
     return out
 
 

@@ -243,8 +243,12 @@ typedef struct pm_render_params {
                                     final_gathering_depth, averaged; 1 is the
                                     reference (integrator.h:224-235)         */
   int32_t spp_batch;             /* samples per pixel per pass, 0 = auto    */
-  int32_t reserved;
+  int32_t flags;                 /* PM_RENDER_FP64_CHECK or 0               */
 } pm_render_params;
+
+/* pm_render_params.flags: also sum every pixel's kept samples in FP64 and
+ * report how far the FP32 image is from those sums (accum_rel_err). */
+#define PM_RENDER_FP64_CHECK 1
 
 typedef struct pm_render_stats {
   int64_t samples;            /* camera samples taken                      */
@@ -254,6 +258,10 @@ typedef struct pm_render_stats {
   int64_t queries_caustics;   /* caustics-map estimates                    */
   int32_t passes;             /* sample batches                            */
   int32_t reserved;
+  double accum_rel_err;       /* with PM_RENDER_FP64_CHECK: the largest
+                                 relative difference, over pixels and
+                                 channels, between the image and the FP64
+                                 sums of the same samples; 0 otherwise     */
 } pm_render_stats;
 
 /* The render loop of examples/main.cpp:33-70 with

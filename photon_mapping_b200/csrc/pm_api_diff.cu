@@ -224,6 +224,7 @@ extern "C" int pm_diff_forward(pm_ctx* c, const pm_camera* cam, const pm_diff_pa
     stats->queries_caustics = q_tot[1];
     stats->passes = 1;
     stats->reserved = 0;
+    stats->accum_rel_err = 0.0;
   }
   return PM_OK;
 }

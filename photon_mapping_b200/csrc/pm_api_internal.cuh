@@ -115,6 +115,7 @@ struct pm_ctx {
   pm::DevBuf dev_err;   // device error word of the kernels (int)
   pm::DevBuf trace_raw, trace_keys, trace_misc;  // photon tracing buffers
   pm::DevBuf r_rng, r_accum, r_slots, r_srec, r_res, r_sort, r_misc;  // render
+  pm::DevBuf r_shadow;  // FP64 per-pixel sums of PM_RENDER_FP64_CHECK
   pm::DevBuf scratch;  // map build scratch
   pm::DevBuf q_in, q_out;  // staging of the host-pointer entry points
   pm::DevBuf counter;      // kCounterRing work counters
@@ -144,7 +145,7 @@ struct pm_ctx {
     trace_keys.release();
     trace_misc.release();
     r_rng.release(); r_accum.release(); r_slots.release(); r_srec.release();
-    r_res.release(); r_sort.release(); r_misc.release();
+    r_res.release(); r_sort.release(); r_misc.release(); r_shadow.release();
     diff.release();
   }
   pm::SceneDev scene_view() const { return pm::scene_view(scene, (int*)dev_err.ptr); }

@@ -1,4 +1,6 @@
 // C ABI of the camera pass: pm_render, pm_integrate, pm_render_path_tracing.
+#include <cstring>
+
 #include "../../include/pm_cuda.h"
 #include "pm_api_internal.cuh"
 #include "pm_api_render.cuh"
@@ -138,6 +140,14 @@ extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
       (e = cudaMemsetAsync(c->dev_err.ptr, 0, 64, st)))
     return cuda_status(c, e, "render init");
   render_rng_init((unsigned long long*)c->r_rng.ptr, p.width, p.height, st);
+  double* shadow = nullptr;
+  if (p.flags & PM_RENDER_FP64_CHECK) {
+    if ((s = c->r_shadow.ensure((size_t)npix * 24)) != PM_OK)
+      return set_err(c, s, "FP64 sums");
+    shadow = (double*)c->r_shadow.ptr;
+    if ((e = cudaMemsetAsync(shadow, 0, (size_t)npix * 24, st)) != cudaSuccess)
+      return cuda_status(c, e, "render init");
+  }
   RenderArgs a = base_args(c, p.width, p.height, q_per_sample, p.final_gathering_depth,
                            p.max_depth, p.n_gather);
   a.cam_pos = v3(cam->position[0], cam->position[1], cam->position[2]);
@@ -157,17 +167,23 @@ extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
                             q_tot, nullptr, nullptr)) != PM_OK)
       return s;
     render_resolve(a.slots, a.sample_rec, (const float*)c->r_res.ptr, npix, b, q_per_sample,
-                   (float4*)c->r_accum.ptr, dropped, st);
+                   (float4*)c->r_accum.ptr, dropped, st, nullptr, shadow);
     ++passes;
   }
   render_finish((const float4*)c->r_accum.ptr, npix, std::max(p.spp, 1), (float*)c->q_out.ptr,
                 st);
+  unsigned* max_bits = (unsigned*)((char*)c->r_misc.ptr + 32);
+  if (shadow)
+    render_shadow_compare((const float*)c->q_out.ptr, shadow, npix, std::max(p.spp, 1),
+                          max_bits, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(c, e, "render");
   unsigned long long hd[2] = {0, 0};
   int herr = 0;
+  unsigned hmax = 0;
   if ((e = cudaMemcpyAsync(out_rgb, c->q_out.ptr, (size_t)npix * 12, cudaMemcpyDeviceToHost,
                            st)) ||
       (e = cudaMemcpyAsync(hd, dropped, 16, cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaMemcpyAsync(&hmax, max_bits, 4, cudaMemcpyDeviceToHost, st)) ||
       (e = cudaMemcpyAsync(&herr, c->dev_err.ptr, 4, cudaMemcpyDeviceToHost, st)) ||
       (e = cudaStreamSynchronize(st)))
     return cuda_status(c, e, "render output");
@@ -183,6 +199,9 @@ extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
     stats->queries_caustics = q_tot[1];
     stats->passes = passes;
     stats->reserved = 0;
+    float mx = 0.f;
+    memcpy(&mx, &hmax, 4);
+    stats->accum_rel_err = shadow ? (double)mx : 0.0;
   }
   return PM_OK;
 }

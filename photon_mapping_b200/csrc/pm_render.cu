@@ -293,7 +293,7 @@ __global__ void resolve_kernel(const float4* __restrict__ slots,
                                int batch, int q_per_sample,
                                float4* __restrict__ accum,
                                unsigned long long* __restrict__ dropped,
-                               float* __restrict__ raw) {
+                               float* __restrict__ raw, double* __restrict__ shadow) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= npix) return;
   float4 acc = raw ? make_float4(0.f, 0.f, 0.f, 0.f) : accum[p];
@@ -312,6 +312,11 @@ __global__ void resolve_kernel(const float4* __restrict__ slots,
     acc.x += rad.x;
     acc.y += rad.y;
     acc.z += rad.z;
+    if (shadow) {
+      shadow[3 * p] += (double)rad.x;
+      shadow[3 * p + 1] += (double)rad.y;
+      shadow[3 * p + 2] += (double)rad.z;
+    }
   }
   if (raw) return;
   accum[p] = acc;
@@ -361,9 +366,33 @@ void render_list_queries(const float4* slots, const float4* srec,
 
 void render_resolve(const float4* slots, const float4* srec, const float* res,
                     int npix, int batch, int q_per_sample, float4* accum,
-                    unsigned long long* dropped, cudaStream_t s, float* raw) {
+                    unsigned long long* dropped, cudaStream_t s, float* raw,
+                    double* shadow) {
   resolve_kernel<<<(npix + 127) / 128, 128, 0, s>>>(
-      slots, srec, res, npix, batch, q_per_sample, accum, dropped, raw);
+      slots, srec, res, npix, batch, q_per_sample, accum, dropped, raw, shadow);
+}
+
+__global__ void shadow_compare_kernel(const float* __restrict__ out,
+                                      const double* __restrict__ shadow, int n, double spp,
+                                      unsigned* __restrict__ max_bits) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  float rel = 0.f;
+  if (i < n) {
+    const double want = shadow[i] / spp;
+    const double d = fabs((double)out[i] - want);
+    const double sc = fabs(want);
+    rel = (float)(sc > 0.0 ? d / sc : d);
+    if (!(rel >= 0.f)) rel = 0.f;  // NaN: pixels of NaN samples are not summed
+  }
+  for (int o = 16; o > 0; o >>= 1) rel = fmaxf(rel, __shfl_xor_sync(kFull, rel, o));
+  if ((threadIdx.x & 31) == 0 && rel > 0.f) atomicMax(max_bits, __float_as_uint(rel));
+}
+
+void render_shadow_compare(const float* out, const double* shadow, int npix, int spp,
+                           unsigned* max_bits, cudaStream_t s) {
+  const int n = 3 * npix;
+  shadow_compare_kernel<<<(n + 255) / 256, 256, 0, s>>>(out, shadow, n,
+                                                        (double)(spp > 0 ? spp : 1), max_bits);
 }
 
 void render_finish(const float4* accum, int npix, int spp, float* out,

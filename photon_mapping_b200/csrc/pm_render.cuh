@@ -51,11 +51,17 @@ void render_list_queries(const float4* slots, const float4* srec,
                          const float* scene_lo, const float* scene_hi,
                          uint32_t* keys, uint32_t* vals, unsigned* count,
                          cudaStream_t s);
-// raw != null: write each sample's radiance there instead of accumulating
+// raw != null: write each sample's radiance there instead of accumulating.
+// shadow != null: also add every kept sample to the pixel's FP64 sums
+// (3 doubles per pixel).
 void render_resolve(const float4* slots, const float4* srec, const float* res,
                     int npix, int batch, int q_per_sample, float4* accum,
                     unsigned long long* dropped, cudaStream_t s,
-                    float* raw = nullptr);
+                    float* raw = nullptr, double* shadow = nullptr);
+// Largest relative difference between out (the image, height x width x 3)
+// and shadow / spp, as float bits in *max_bits (atomicMax; start it at 0).
+void render_shadow_compare(const float* out, const double* shadow, int npix, int spp,
+                           unsigned* max_bits, cudaStream_t s);
 void render_finish(const float4* accum, int npix, int spp, float* out,
                    cudaStream_t s);
 

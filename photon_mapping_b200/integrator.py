@@ -18,16 +18,22 @@ class RenderParams(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("spp", C.c_int32),
                 ("k_global", C.c_int32), ("k_caustics", C.c_int32),
                 ("final_gathering_depth", C.c_int32), ("max_depth", C.c_int32),
-                ("n_gather", C.c_int32), ("spp_batch", C.c_int32), ("reserved", C.c_int32)]
+                ("n_gather", C.c_int32), ("spp_batch", C.c_int32), ("flags", C.c_int32)]
+
+PM_RENDER_FP64_CHECK = 1
 
 
 class RenderStats(C.Structure):
     _fields_ = [("samples", C.c_int64), ("dropped_nan", C.c_int64),
                 ("dropped_negative", C.c_int64), ("queries_global", C.c_int64),
-                ("queries_caustics", C.c_int64), ("passes", C.c_int32), ("reserved", C.c_int32)]
+                ("queries_caustics", C.c_int64), ("passes", C.c_int32), ("reserved", C.c_int32),
+                ("accum_rel_err", C.c_double)]
 
     def as_dict(self) -> dict:
-        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "reserved"}
+        d = {k: int(getattr(self, k)) for k, _ in self._fields_
+             if k not in ("reserved", "accum_rel_err")}
+        d["accum_rel_err"] = float(self.accum_rel_err)
+        return d
 
 
 class IntegrateParams(C.Structure):
@@ -113,15 +119,18 @@ class PhotonMapping:
         return out[0]
 
     def render(self, camera, width: int, height: int, n_samples: int, n_gather: int = 1,
-               spp_batch: int = 0):
+               spp_batch: int = 0, fp64_check: bool = False):
         """The render loop of examples/main.cpp:33-70 on the device: returns
         (image (height, width, 3) float32 averaged over n_samples, stats).
         The caustics estimate uses k = nEstimationGlobal like the reference
-        (integrator.h:161)."""
+        (integrator.h:161). fp64_check: also sum the samples in FP64 and
+        report the image's largest relative difference from those sums
+        (stats["accum_rel_err"])."""
         import numpy as np
         p = RenderParams(int(width), int(height), int(n_samples), self.nEstimationGlobal,
                          self.nEstimationGlobal, self.finalGatheringDepth, self.maxDepth,
-                         int(n_gather), int(spp_batch), 0)
+                         int(n_gather), int(spp_batch),
+                         PM_RENDER_FP64_CHECK if fp64_check else 0)
         out = np.empty((height, width, 3), np.float32)
         st = RenderStats()
         cam = camera.as_struct()

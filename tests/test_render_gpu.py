@@ -200,3 +200,20 @@ def test_path_tracing_matches_reference_integrator(ctx, tmp_path):
     np.testing.assert_allclose(got, want, rtol=1e-3, atol=1e-6)
     rel = np.abs(got - want) / np.maximum(np.abs(want), 1e-6)
     assert (rel > 1e-5).mean() < 5e-3
+
+
+def test_fp64_accumulation_check(ctx):
+    """PM_RENDER_FP64_CHECK: the same image, and the FP32 per-pixel sums
+    within float rounding of FP64 sums of the same samples."""
+    mesh = S.cornell_box(0)
+    pmi = setup(ctx, mesh, 30000, 40, 1, 100)
+    cam = Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
+    plain, st0 = pmi.render(cam, 48, 40, 16)
+    img, st = pmi.render(cam, 48, 40, 16, fp64_check=True)
+    np.testing.assert_array_equal(img, plain)
+    assert st0["accum_rel_err"] == 0.0
+    assert 0.0 < st["accum_rel_err"] < 1e-5
+    # several passes accumulate into the same sums
+    img2, st2 = pmi.render(cam, 48, 40, 16, spp_batch=3, fp64_check=True)
+    np.testing.assert_array_equal(img2, plain)
+    assert st2["passes"] == 6 and st2["accum_rel_err"] < 1e-5
