@@ -11,6 +11,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -32,6 +33,7 @@ constexpr int kSideStreams = 8;
 }  // namespace
 
 struct pm_batch {
+  std::mutex mu;  // calls on one batch are serialised
   int device = 0, num_sms = 148;
   cudaStream_t st = nullptr;
   cudaStream_t side[kSideStreams] = {};
@@ -395,6 +397,8 @@ int plan(pm_batch* b) {
   return PM_OK;
 }
 
+int set_tuning(pm_batch* b, const pm_batch_tuning* t);
+
 }  // namespace
 
 extern "C" {
@@ -496,6 +500,16 @@ const char* pm_batch_last_error(const pm_batch* b) { return b ? b->err.c_str() :
 
 int pm_batch_set_tuning(pm_batch* b, const pm_batch_tuning* t) {
   if (!b) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
+  return set_tuning(b, t);
+}
+
+}  // extern "C"
+
+namespace {
+
+// pm_batch_set_tuning with the batch's lock held.
+int set_tuning(pm_batch* b, const pm_batch_tuning* t) {
   if (!t || !tuning_ok(b, *t)) return berr(b, PM_ERR_INVALID_ARGUMENT, "tuning out of range");
   cudaSetDevice(b->device);
   cudaError_t e;
@@ -511,14 +525,20 @@ int pm_batch_set_tuning(pm_batch* b, const pm_batch_tuning* t) {
   return PM_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
 int pm_batch_get_tuning(pm_batch* b, pm_batch_tuning* t) {
   if (!b || !t) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
   *t = b->tune;
   return PM_OK;
 }
 
 int pm_batch_render(pm_batch* b, int32_t use_graph, float* ms) {
   if (!b) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->device);
   cudaError_t e;
   if (use_graph && !b->exec) {
@@ -555,6 +575,7 @@ int pm_batch_render(pm_batch* b, int32_t use_graph, float* ms) {
 
 int pm_batch_autotune(pm_batch* b, pm_batch_tuning* best, float* ms_stage) {
   if (!b) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
   cudaSetDevice(b->device);
   cudaError_t e;
   int s;
@@ -628,7 +649,7 @@ int pm_batch_autotune(pm_batch* b, pm_batch_tuning* best, float* ms_stage) {
           t.knn_buffer = bf;
         }
       }
-  if ((s = pm_batch_set_tuning(b, &t)) != PM_OK) return s;
+  if ((s = set_tuning(b, &t)) != PM_OK) return s;
   if (best) *best = t;
   if (ms_stage) {
     ms_stage[0] = best_trace;
@@ -642,6 +663,7 @@ int pm_batch_autotune(pm_batch* b, pm_batch_tuning* best, float* ms_stage) {
 
 int pm_batch_image(pm_batch* b, int32_t scene, float* out) {
   if (!b) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
   if (scene < 0 || scene >= b->n || !out) return berr(b, PM_ERR_INVALID_ARGUMENT, "scene / out");
   cudaSetDevice(b->device);
   const int64_t px = b->pix_off[scene + 1] - b->pix_off[scene];
@@ -655,6 +677,7 @@ int pm_batch_image(pm_batch* b, int32_t scene, float* out) {
 
 int pm_batch_counts(pm_batch* b, int64_t* stored, int64_t* queries) {
   if (!b) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
   for (int s = 0; s < b->n; ++s) {
     if (stored) stored[s] = b->stored[s];
     if (queries) queries[s] = b->queries[s];
