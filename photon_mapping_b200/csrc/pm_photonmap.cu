@@ -252,7 +252,7 @@ struct WarpBuf {
   uint32_t id[C];   // sorted position of the photon
   uint32_t hist[256];
   uint32_t stack[kStack];
-  uint32_t list[32];  // passing groups of the node being scanned
+  uint32_t list[64];  // passing groups waiting to be scanned, in walk order
   uint32_t sel[32];   // entries of the critical bin of a selection
   uint32_t stat[8];   // per-warp counters, same order as pm_knn_stats
 };
@@ -631,7 +631,7 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
   }
   const int top = m.nlevels - 1;
   if (lane == 0) s.stack[0] = ((uint32_t)top << 28);
-  int sp = 1;
+  int sp = 1, pending = 0;
   __syncwarp();
   while (sp > 0) {
     --sp;
@@ -650,9 +650,23 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
     }
     const unsigned bal = __ballot_sync(kFull, pass);
     if (cl == 0) {
-      if (pass) s.list[__popc(bal & lanemask_lt())] = (uint32_t)c;
+      // the passing groups join the waiting list; full rounds of 8 groups
+      // are scanned, the rest waits for the next node (the scan order stays
+      // the walk's order)
+      if (pass) s.list[pending + __popc(bal & lanemask_lt())] = (uint32_t)c;
+      pending += __popc(bal);
       __syncwarp();
-      if (bal) scan_groups<C, S>(m, q, s, lane, __popc(bal));
+      if (pending >= 8) {
+        const int full = pending & ~7;
+        scan_groups<C, S>(m, q, s, lane, full);
+        const int rest = pending - full;
+        uint32_t keep = 0;
+        if (lane < rest) keep = s.list[full + lane];
+        __syncwarp();
+        if (lane < rest) s.list[lane] = keep;
+        __syncwarp();
+        pending = rest;
+      }
     } else {
       if (pass)
         s.stack[sp + __popc(bal & lanemask_lt())] = ((uint32_t)cl << 28) | c;
@@ -660,6 +674,7 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
       __syncwarp();
     }
   }
+  if (pending) scan_groups<C, S>(m, q, s, lane, pending);
 }
 
 __device__ __forceinline__ unsigned long long warp_min_u64(
