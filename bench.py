@@ -581,7 +581,9 @@ def run_ours(args) -> None:
         "config": config_dict(nq, int(photons.shape[0])),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                     "peak_source": ("measured (MEASURED_PEAKS.json hbm_gbs)"
+                                     if peak_kind == "measured" else
+                                     "fallback 6650 GB/s (MEASURED_PEAKS.json absent)"),
                      "bytes_per_query": BYTES_PER_QUERY},
         "cpu_baseline": cpu,
         "e2e": {"value": e2e_value, "unit": "queries/s",

@@ -244,7 +244,15 @@ constexpr int kStack = 32 * kMaxLevels;
 // queries: 123 candidates per query at k = 100 against 181 with the sure
 // bound alone).
 constexpr float kWarmGuess = 1.06f;
-constexpr int kChunk = 32;  // queries a warp takes per work-counter bump
+// Work items of the persistent launch: kChunk consecutive queries per
+// work-counter bump, then kTail queries per bump for the last
+// kTailItems x (resident warps) x kTail queries, so that the warps run out
+// of work at nearly the same time (measured on 1M primary-hit queries at
+// k = 100: 3.68 ms against 3.96 ms with items of 32 throughout; larger
+// items keep more warm starts but leave a longer tail).
+constexpr int kChunk = 16;
+constexpr int kTail = 8;
+constexpr int kTailItems = 2;
 
 template <int C>
 struct WarpBuf {
@@ -959,7 +967,7 @@ __global__ void __launch_bounds__(256, 4)
     knn_kernel(MapDev m, const void* __restrict__ queries, int64_t nq, int k,
                float n_emitted, KnnOut out,
                unsigned long long* __restrict__ counter,
-               const uint32_t* __restrict__ order, int stride4) {
+               const uint32_t* __restrict__ order, int stride4, int64_t head_items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ Levels L;
   WarpBuf<C>& s = reinterpret_cast<WarpBuf<C>*>(smem_raw)[threadIdx.x >> 5];
@@ -979,9 +987,11 @@ __global__ void __launch_bounds__(256, 4)
     unsigned long long c0 = 0;
     if (lane == 0) c0 = atomicAdd(counter, 1ull);
     c0 = __shfl_sync(kFull, c0, 0);
-    const int64_t qb = (int64_t)c0 * kChunk;
+    const int64_t item = (int64_t)c0;  // items [0, head_items) hold kChunk queries
+    const bool head = item < head_items;
+    const int64_t qb = head ? item * kChunk : head_items * kChunk + (item - head_items) * kTail;
     if (qb >= nq) break;
-    const int64_t qe = min(nq, qb + kChunk);
+    const int64_t qe = min(nq, qb + (head ? kChunk : kTail));
 
     knn_chunk<C, MODE, S>(m, L, s, lane, queries, qb, qe, k, n_emitted, out, order, stride4,
                           r_hint);
@@ -1013,16 +1023,18 @@ static cudaError_t launch_one(const MapDev& m, const void* queries,
                                                     smem);
   if (e != cudaSuccess) return e;
   if (per_sm < 1) per_sm = 1;
-  const int64_t chunks = (nq + kChunk - 1) / kChunk;
+  const int64_t chunks = (nq + kTail - 1) / kTail;
   const int64_t warps_per_block = kThreads / 32;
   int64_t blocks = (int64_t)num_sms * per_sm;
   const int64_t need = (chunks + warps_per_block - 1) / warps_per_block;
   if (blocks > need) blocks = need;
   if (blocks < 1) blocks = 1;
+  const int64_t tail = blocks * warps_per_block * kTail * kTailItems;
+  const int64_t head_items = nq > tail ? (nq - tail) / kChunk : 0;
   e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
   kern<<<(unsigned)blocks, kThreads, smem, st>>>(m, queries, nq, k, n_emitted,
-                                                 out, counter, order, stride4);
+                                                 out, counter, order, stride4, head_items);
   return cudaGetLastError();
 }
 
