@@ -359,18 +359,27 @@ int pm_photonmap_radiance(pm_ctx* c, int map, const pm_radiance_query* q,
   if (nq == 0) return PM_OK;
   const size_t qb = (size_t)nq * sizeof(pm_radiance_query);
   const size_t ob = (size_t)nq * 3 * sizeof(float);
-  int s;
-  if ((s = c->q_in.ensure(qb)) || (s = c->q_out.ensure(ob)))
-    return set_err(c, s, "query buffers");
   cudaStream_t st = c->stream;
-  cudaError_t e = copy_in(c->q_in.ptr, q, qb, c->num_sms, st);
-  if (e != cudaSuccess) return cuda_status(c, e, "query upload");
+  cudaError_t e;
+  // A mapped, 16-byte aligned query buffer is read in place by the kernel
+  // (each record is fetched one query ahead, so the host-memory latency
+  // overlaps the previous query's search); others are copied first.
+  const void* d_q = mapped_host(q);
+  if (d_q && ((uintptr_t)d_q & 15) != 0) d_q = nullptr;
   // a mapped output buffer is written by the kernel itself
   float* mapped_out = (float*)mapped_host(out_rgb);
+  int s = PM_OK;
+  if ((!d_q && (s = c->q_in.ensure(qb))) || (!mapped_out && (s = c->q_out.ensure(ob))))
+    return set_err(c, s, "query buffers");
+  if (!d_q) {
+    e = copy_in(c->q_in.ptr, q, qb, c->num_sms, st);
+    if (e != cudaSuccess) return cuda_status(c, e, "query upload");
+    d_q = c->q_in.ptr;
+  }
   KnnOut o{};
   o.stats = c->stats_ptr();
   o.rgb = mapped_out ? mapped_out : (float*)c->q_out.ptr;
-  e = knn_launch(map_view(dm), c->q_in.ptr, nq, k, kModeRadiance,
+  e = knn_launch(map_view(dm), d_q, nq, k, kModeRadiance,
                  (float)n_emitted, o, c->next_counter(), c->num_sms, st);
   if (e != cudaSuccess) return cuda_status(c, e, "radiance launch");
   if (!mapped_out) {

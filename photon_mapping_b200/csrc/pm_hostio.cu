@@ -4,9 +4,11 @@
 // at about 24 GB/s, while kernels reading the same memory through its
 // device mapping reached about 55 GB/s (PCIe 5.0 x16). So when a caller's
 // buffer is page-locked and mapped (cudaPointerGetAttributes: host memory
-// with a device address), inputs are fetched by a streaming copy kernel and
-// outputs are written by the compute kernel straight into the host buffer;
-// other (pageable) buffers go through cudaMemcpyAsync.
+// with a device address), outputs are written by the compute kernel straight
+// into the host buffer, and inputs are either read in place by the compute
+// kernel (the radiance estimate, which fetches each query record one query
+// ahead) or fetched by a streaming copy kernel (the index search); other
+// (pageable) buffers go through cudaMemcpyAsync.
 #include "pm_hostio.cuh"
 
 namespace pm {

@@ -253,6 +253,13 @@ constexpr float kWarmGuess = 1.06f;
 constexpr int kChunk = 16;
 constexpr int kTail = 8;
 constexpr int kTailItems = 2;
+static_assert(kChunk % 8 == 0 && kTail % 8 == 0, "items start at multiples of 8");
+
+// The last kStageWords entries of WarpBuf::id hold the radiance of up to 8
+// consecutive queries (an aligned group of 8) until the warp stores them
+// together: 96 bytes in six 16-byte stores instead of 24 scattered words,
+// which matters when the output is mapped host memory.
+constexpr int kStageWords = 24;
 
 template <int C>
 struct WarpBuf {
@@ -263,7 +270,21 @@ struct WarpBuf {
   uint32_t list[64];  // passing groups waiting to be scanned, in walk order
   uint32_t sel[32];   // entries of the critical bin of a selection
   uint32_t stat[8];   // per-warp counters, same order as pm_knn_stats
+  float4 rec[2][3];   // radiance records of this query and the next (cp.async)
 };
+
+// 16-byte asynchronous copy global -> shared (the source may be mapped host
+// memory), and the waits on it (per thread).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
 
 struct Levels {
   int off[kMaxLevels];
@@ -578,7 +599,7 @@ __device__ __forceinline__ void offer(const MapDev& m, Query& q, WarpBuf<C>& s,
     s.id[o] = (uint32_t)i;
   }
   q.cnt += __popc(bal);
-  if (q.cnt > C - 32) {
+  if (q.cnt > C - 32 - kStageWords) {
     __syncwarp();
     const uint2 r = tighten<C, S>(m.pos4, &s, q.cnt, q.k, q.tau, lane);
     q.cnt = (int)r.x;
@@ -756,17 +777,31 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
   const float kInf = __int_as_float(0x7f800000);
   bool have_prev = false;
   float pqx = 0.f, pqy = 0.f, pqz = 0.f, pkth = 0.f;
-  for (int64_t qi = qb; qi < qe; ++qi) {
+  // The three float4 of a radiance record are staged in s.rec by lanes 0-2
+  // one query ahead, so the load (from device or mapped host memory)
+  // overlaps the previous query's search.
+  auto fetch = [&](int64_t qn, int b) {
+    if (lane < 3) {
+      const int64_t rn = order ? (int64_t)__ldg(order + qn) : qn;
+      cp_async16(&s.rec[b][lane], reinterpret_cast<const float4*>(queries) + stride4 * rn + lane);
+    }
+    cp_async_commit();
+  };
+  int buf = 0;
+  if (MODE != kModeKnn) fetch(qb, 0);
+  for (int64_t qi = qb; qi < qe; ++qi, buf ^= 1) {
     Query q;
     q.k = k;
     q.cnt = 0;
     q.tau = kInf;
     const int64_t rec = (MODE != kModeKnn && order) ? (int64_t)__ldg(order + qi) : qi;
     if (MODE != kModeKnn) {
-      // radiance record r0 = {pos, rho.r}; wo, ns and the other albedo
-      // channels are read after the search
-      const float4 r0 =
-          __ldg(reinterpret_cast<const float4*>(queries) + stride4 * rec);
+      cp_async_wait_all();
+      __syncwarp();  // this record is visible; every lane is done with the other buffer
+      if (qi + 1 < qe) fetch(qi + 1, buf ^ 1);
+      // r0 = {pos, rho.r}; wo, ns and the other albedo channels are read
+      // after the search
+      const float4 r0 = s.rec[buf][0];
       q.x = r0.x; q.y = r0.y; q.z = r0.z;
     } else {
       const float* q3 = reinterpret_cast<const float*>(queries) + 3 * qi;
@@ -858,11 +893,9 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
     if (MODE == kModeAdjoint) {
       // d estimate / d throughput_i = f(wo, wi_i) / (n_emitted pi maxd2)
       // for the kept photons (integrator.h:141-150)
-      const float4* q4 =
-          reinterpret_cast<const float4*>(queries) + stride4 * rec;
-      const float4 r0 = __ldg(q4);
-      const float4 r1 = __ldg(q4 + 1);
-      const float4 r2 = __ldg(q4 + 2);
+      const float4 r0 = s.rec[buf][0];
+      const float4 r1 = s.rec[buf][1];
+      const float4 r2 = s.rec[buf][2];
       const float ax = out.adj_in[3 * rec], ay = out.adj_in[3 * rec + 1],
                   az = out.adj_in[3 * rec + 2];
       const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
@@ -883,11 +916,9 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
       }
     } else if (MODE == kModeRadiance) {
       // r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b}
-      const float4* q4 =
-          reinterpret_cast<const float4*>(queries) + stride4 * rec;
-      const float4 r0 = __ldg(q4);
-      const float4 r1 = __ldg(q4 + 1);
-      const float4 r2 = __ldg(q4 + 2);
+      const float4 r0 = s.rec[buf][0];
+      const float4 r1 = s.rec[buf][1];
+      const float4 r2 = s.rec[buf][2];
       const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
       const float fr = __fdiv_rn(r0.w, kPI);
       const float fg = __fdiv_rn(r1.w, kPI);
@@ -923,9 +954,29 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
           o3 = make_float3(__fdiv_rn(lr, den), __fdiv_rn(lg, den),
                            __fdiv_rn(lb, den));
         }
-        out.rgb[3 * rec + 0] = o3.x;
-        out.rgb[3 * rec + 1] = o3.y;
-        out.rgb[3 * rec + 2] = o3.z;
+        if (!order) {
+          float* r = reinterpret_cast<float*>(s.id + C - kStageWords) + 3 * (qi & 7);
+          r[0] = o3.x; r[1] = o3.y; r[2] = o3.z;
+        } else {
+          out.rgb[3 * rec + 0] = o3.x;
+          out.rgb[3 * rec + 1] = o3.y;
+          out.rgb[3 * rec + 2] = o3.z;
+        }
+      }
+      // work items without `order` start at multiples of 8: a group of 8 is
+      // complete at qi % 8 == 7 or cut by the end of the queries
+      if (!order && ((qi & 7) == 7 || qi + 1 == qe)) {
+        __syncwarp();
+        const int64_t g0 = qi & ~(int64_t)7;
+        const int nf = 3 * (int)(qi + 1 - g0);
+        float* dst = out.rgb + 3 * g0;
+        const float* src = reinterpret_cast<const float*>(s.id + C - kStageWords);
+        if (nf == kStageWords && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+          if (lane < kStageWords / 4)
+            reinterpret_cast<float4*>(dst)[lane] = reinterpret_cast<const float4*>(src)[lane];
+        } else if (lane < nf) {
+          dst[lane] = src[lane];
+        }
       }
     } else {
       int n2 = cnt;

@@ -177,9 +177,11 @@ def test_large_map_properties(ctx):
 
 
 def test_page_locked_host_buffers(ctx):
-    """Host-pointer calls with page-locked (mapped) buffers fetch the
-    queries with a copy kernel and write the results straight into the
-    host buffers; the results equal those of pageable buffers."""
+    """Host-pointer calls with page-locked (mapped) buffers read the
+    radiance queries in place (the index search: through a copy kernel) and
+    write the results straight into the host buffers; the results equal
+    those of pageable buffers, also for buffers that start off a 16-byte
+    boundary and for a query count that is not a multiple of 8."""
     import ctypes as C
     import torch
     ph = W.wall_photons(100000, seed=7)
@@ -208,3 +210,22 @@ def test_page_locked_host_buffers(ctx):
     ctx.check(ctx.lib.pm_photonmap_knn(ctx.handle, 0, hp1.data_ptr(), 5, 30, i1.ctypes.data,
                                        c1.ctypes.data, m1.ctypes.data), "pm_photonmap_knn")
     np.testing.assert_array_equal(i1, widx[:5])
+    # mapped buffers 4 bytes off a 16-byte boundary: the queries are copied
+    # first, the results are stored word by word
+    n = q.shape[0]
+    qbig = torch.zeros(q.size + 1, dtype=torch.float32).pin_memory()
+    qbig[1:] = torch.from_numpy(np.ascontiguousarray(q).reshape(-1))
+    obig = torch.zeros(3 * n + 1, dtype=torch.float32).pin_memory()
+    ctx.check(ctx.lib.pm_photonmap_radiance(ctx.handle, 0, qbig[1:].data_ptr(), n, 50, 100000,
+                                            obig[1:].data_ptr()), "pm_photonmap_radiance")
+    np.testing.assert_array_equal(obig[1:].numpy().reshape(n, 3), want)
+    assert obig[0].item() == 0.0
+    # device buffers, output 4 bytes off a 16-byte boundary
+    dq = torch.from_numpy(np.ascontiguousarray(q)).cuda()
+    dout = torch.zeros(3 * n + 1, dtype=torch.float32, device="cuda")
+    ctx.check(ctx.lib.pm_photonmap_radiance_device(ctx.handle, 0, dq.data_ptr(), n, 50, 100000,
+                                                   dout[1:].data_ptr(), None),
+              "pm_photonmap_radiance_device")
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(dout[1:].cpu().numpy().reshape(n, 3), want)
+    assert dout[0].item() == 0.0
