@@ -72,7 +72,7 @@ def scene_and_camera():
 def config_dict(nq: int, n_stored: int) -> dict:
     return {
         "workload": (f"radiance estimate k={K_NEAREST} on the photon map traced from {N_EMIT} "
-                     f"emitted photons in the procedural Cornell box (configs[1] scene); queries = "
+                     f"emitted photons in the procedural Cornell box (512x512 frame scene); queries = "
                      f"primary hits of a {IMAGE_W}x{IMAGE_H}x{SPP}spp frame in pixel order"),
         "photons_emitted": N_EMIT,
         "photons_stored": n_stored,
@@ -214,21 +214,22 @@ def cpu_reference_rate(photons, queries, n_queries: int, repeats: int = 1):
 # ---------------------------------------------------------------- render rates
 
 RENDER_CONFIGS = {
-    # configs[0]: 256^2, 100k photons, k=100, 16 spp, no final gathering
-    "config1": dict(width=256, height=256, spp=16, photons=100_000, k=100, fg=0, n_gather=1),
-    # 512^2, 1M photons, k=100, final gathering with 16 gather rays;
-    # timed on 2 of its 100 spp (samples/s is per sample)
-    "config2": dict(width=512, height=512, spp=2, photons=1_000_000, k=100, fg=1, n_gather=16),
+    # 256^2, 100k photons, k=100, 16 spp, no final gathering
+    "cornell_256_100k_direct": dict(width=256, height=256, spp=16, photons=100_000, k=100, fg=0, n_gather=1),
+    # 512^2, 1M photons, k=100, final gathering with 16 gather rays; timed on
+    # 2 of the setting's 100 spp (samples/s is per sample)
+    "cornell_512_1M_fg16": dict(width=512, height=512, spp=2, photons=1_000_000, k=100, fg=1, n_gather=16),
     # the same with the reference integrator's single gather ray per hit
     # (integrator.h:292-309), the setting its CPU time is taken on
-    "config2_gather1": dict(width=512, height=512, spp=4, photons=1_000_000, k=100, fg=1,
+    "cornell_512_1M_fg1": dict(width=512, height=512, spp=4, photons=1_000_000, k=100, fg=1,
                             n_gather=1),
-    # caustics scene (mirror and glass icospheres, 512x512 water
-    # heightfield; 563,238 triangles), 1M global + 10M caustics photons,
-    # k=100, final gathering; timed on 2 of its 64 spp
-    "config3": dict(width=512, height=512, spp=2, photons=1_000_000, k=100, fg=1, n_gather=1,
+    # caustics scene (mirror and glass icospheres, 512x512 water heightfield;
+    # 563,238 triangles), 1M global + 10M caustics photons, k=100, final
+    # gathering; timed on 2 of the setting's 64 spp
+    "caustics_512_11M_fg1": dict(width=512, height=512, spp=2, photons=1_000_000, k=100, fg=1, n_gather=1,
                     scene="caustics", caustics_multiplier=10.0),
 }
+RENDER_REPEATS = 3           # timed renders per setting (median reported)
 CPU_RENDER_BUDGET_S = 6.0   # per config, for the reference integrator's bounded sample
 
 
@@ -287,13 +288,18 @@ def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
             t0 = time.perf_counter()
             trace = pmi.build(scene_dev, seed=TRACE_SEED)
             trace_s = time.perf_counter() - t0
-        pmi.render(camera, c["width"], c["height"], 1, n_gather=c["n_gather"])  # warm-up
-        torch.cuda.synchronize(dev)
-        t0 = time.perf_counter()
-        img, st = pmi.render(camera, c["width"], c["height"], c["spp"], n_gather=c["n_gather"])
-        dt = time.perf_counter() - t0
+        # warm-up at the same setting (the render buffers reach their size)
+        pmi.render(camera, c["width"], c["height"], c["spp"], n_gather=c["n_gather"])
+        times = []
+        for _ in range(RENDER_REPEATS):
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            img, st = pmi.render(camera, c["width"], c["height"], c["spp"],
+                                 n_gather=c["n_gather"])
+            times.append(time.perf_counter() - t0)
+        dt = statistics.median(times)
         n = c["width"] * c["height"] * c["spp"]
-        out[name] = {"samples_per_s": n / dt, "seconds": dt, **c,
+        out[name] = {"samples_per_s": n / dt, "seconds": dt, "repeats": RENDER_REPEATS, **c,
                      "queries_global": st["queries_global"],
                      "queries_caustics": st["queries_caustics"], "passes": st["passes"],
                      "mean_radiance": float(img.mean())}
@@ -312,7 +318,7 @@ def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
 
 # ------------------------------------------------------------------ gradients
 
-# the config-1 Cornell box at 256^2, 1M photons, k = 50, final
+# The Cornell box at 256^2, 1M photons, k = 50, final
 # gathering, 16 spp; loss = MSE against a render with seed-perturbed albedos
 # (8 materials x RGB) and emission
 GRAD_CONFIG = dict(width=256, height=256, spp=16, photons=1_000_000, k=50, fg=1, n_gather=1)
@@ -365,7 +371,7 @@ def gradient_rates(ctx, mesh, camera, dev) -> dict:
     g = np.concatenate([ga, ge[None]])
     fd_err = max(abs(g[p, ch] - fd[p, ch]) / max(abs(fd[p, ch]), 1e-30) for p, ch in which)
     return {
-        "workload": ("configs[3]: Cornell box (8 material albedos x RGB + emission RGB = 27 "
+        "workload": ("Cornell box (8 material albedos x RGB + emission RGB = 27 "
                      f"parameters), {c['width']}x{c['height']}, {c['spp']} spp, "
                      f"{c['photons']} photons, k={c['k']}, final gathering; MSE loss against "
                      "a render with seed-perturbed parameters"),
@@ -388,7 +394,7 @@ BATCH_STEPS = 3
 
 
 def batched_rates(n_scenes: int, dev) -> dict:
-    """configs[4]: n_scenes random scenes rendered as one batch (one step =
+    """n_scenes random scenes rendered as one batch (one step =
     every scene's photon trace, map build, camera pass, kNN estimates and
     resolve; CUDA graph, autotuned launch shapes) against the per-scene
     sequential loop over the same scenes; the images must be identical."""
@@ -424,7 +430,7 @@ def batched_rates(n_scenes: int, dev) -> dict:
     seq_step = sum(seq_s) / len(seq_s)
     tris = [sc["mesh"].n_faces for sc in scenes]
     return {
-        "workload": (f"configs[4]: {n_scenes} random Cornell variants (1-40 boxes, displaced "
+        "workload": (f"{n_scenes} random Cornell variants (1-40 boxes, displaced "
                      "heightfield floor, triangles log-uniform 1k-500k), photons log-uniform "
                      "100k-4M, k in {50,100}, square images side log-uniform 128-1024, "
                      f"{scenes[0]['spp']} spp, photon-map estimate at the first diffuse hit"),

@@ -768,7 +768,13 @@ __device__ __forceinline__ float cold_tau(const float4* pos4, const float4* boxe
 
 // Answers queries [qb, qe) of a work item on map m, one at a time (one warp).
 // r_hint: the last exact k-th distance this warp found (in/out).
-template <int C, int MODE, bool S>
+// HIO (the single-map kernel, whose queries and output may be mapped host
+// memory): radiance records are prefetched one query ahead with cp.async,
+// and without `order` the radiance goes out in aligned groups of 8 queries.
+// Without HIO (the batched kernel, device-resident slots) records are read
+// with plain loads: measured on the 64-scene batch, the prefetch and the
+// staging code together cost it 13 % through register allocation.
+template <int C, int MODE, bool S, bool HIO>
 __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, WarpBuf<C>& s,
                                           int lane, const void* __restrict__ queries,
                                           int64_t qb, int64_t qe, int k, float n_emitted,
@@ -777,8 +783,8 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
   const float kInf = __int_as_float(0x7f800000);
   bool have_prev = false;
   float pqx = 0.f, pqy = 0.f, pqz = 0.f, pkth = 0.f;
-  // The three float4 of a radiance record are staged in s.rec by lanes 0-2
-  // one query ahead, so the load (from device or mapped host memory)
+  // HIO: the three float4 of a radiance record are staged in s.rec by lanes
+  // 0-2 one query ahead, so the load (from device or mapped host memory)
   // overlaps the previous query's search.
   auto fetch = [&](int64_t qn, int b) {
     if (lane < 3) {
@@ -788,14 +794,17 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
     cp_async_commit();
   };
   int buf = 0;
-  if (MODE != kModeKnn) fetch(qb, 0);
+  if (MODE != kModeKnn && HIO) fetch(qb, 0);
   for (int64_t qi = qb; qi < qe; ++qi, buf ^= 1) {
     Query q;
     q.k = k;
     q.cnt = 0;
     q.tau = kInf;
     const int64_t rec = (MODE != kModeKnn && order) ? (int64_t)__ldg(order + qi) : qi;
-    if (MODE != kModeKnn) {
+    if (MODE != kModeKnn && !HIO) {
+      const float4 r0 = __ldg(reinterpret_cast<const float4*>(queries) + stride4 * rec);
+      q.x = r0.x; q.y = r0.y; q.z = r0.z;
+    } else if (MODE != kModeKnn) {
       cp_async_wait_all();
       __syncwarp();  // this record is visible; every lane is done with the other buffer
       if (qi + 1 < qe) fetch(qi + 1, buf ^ 1);
@@ -893,9 +902,10 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
     if (MODE == kModeAdjoint) {
       // d estimate / d throughput_i = f(wo, wi_i) / (n_emitted pi maxd2)
       // for the kept photons (integrator.h:141-150)
-      const float4 r0 = s.rec[buf][0];
-      const float4 r1 = s.rec[buf][1];
-      const float4 r2 = s.rec[buf][2];
+      const float4* q4 = reinterpret_cast<const float4*>(queries) + stride4 * rec;
+      const float4 r0 = HIO ? s.rec[buf][0] : __ldg(q4);
+      const float4 r1 = HIO ? s.rec[buf][1] : __ldg(q4 + 1);
+      const float4 r2 = HIO ? s.rec[buf][2] : __ldg(q4 + 2);
       const float ax = out.adj_in[3 * rec], ay = out.adj_in[3 * rec + 1],
                   az = out.adj_in[3 * rec + 2];
       const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
@@ -916,9 +926,10 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
       }
     } else if (MODE == kModeRadiance) {
       // r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b}
-      const float4 r0 = s.rec[buf][0];
-      const float4 r1 = s.rec[buf][1];
-      const float4 r2 = s.rec[buf][2];
+      const float4* q4 = reinterpret_cast<const float4*>(queries) + stride4 * rec;
+      const float4 r0 = HIO ? s.rec[buf][0] : __ldg(q4);
+      const float4 r1 = HIO ? s.rec[buf][1] : __ldg(q4 + 1);
+      const float4 r2 = HIO ? s.rec[buf][2] : __ldg(q4 + 2);
       const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
       const float fr = __fdiv_rn(r0.w, kPI);
       const float fg = __fdiv_rn(r1.w, kPI);
@@ -954,7 +965,7 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
           o3 = make_float3(__fdiv_rn(lr, den), __fdiv_rn(lg, den),
                            __fdiv_rn(lb, den));
         }
-        if (!order) {
+        if (HIO && !order) {
           float* r = reinterpret_cast<float*>(s.id + C - kStageWords) + 3 * (qi & 7);
           r[0] = o3.x; r[1] = o3.y; r[2] = o3.z;
         } else {
@@ -965,7 +976,7 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
       }
       // work items without `order` start at multiples of 8: a group of 8 is
       // complete at qi % 8 == 7 or cut by the end of the queries
-      if (!order && ((qi & 7) == 7 || qi + 1 == qe)) {
+      if (HIO && !order && ((qi & 7) == 7 || qi + 1 == qe)) {
         __syncwarp();
         const int64_t g0 = qi & ~(int64_t)7;
         const int nf = 3 * (int)(qi + 1 - g0);
@@ -1044,7 +1055,7 @@ __global__ void __launch_bounds__(256, 4)
     if (qb >= nq) break;
     const int64_t qe = min(nq, qb + (head ? kChunk : kTail));
 
-    knn_chunk<C, MODE, S>(m, L, s, lane, queries, qb, qe, k, n_emitted, out, order, stride4,
+    knn_chunk<C, MODE, S, true>(m, L, s, lane, queries, qb, qe, k, n_emitted, out, order, stride4,
                           r_hint);
     if (S) {
       __syncwarp();
@@ -1166,7 +1177,7 @@ __global__ void __launch_bounds__(256, 4)
     }
     const int64_t qb = qoff[sc] + ((int64_t)c0 - ioff[sc]) * chunk;
     const int64_t qe = min(qoff[sc + 1], qb + chunk);
-    knn_chunk<C, kModeRadiance, false>(wmap[warp], wlev[warp], s, lane, slots, qb, qe, k,
+    knn_chunk<C, kModeRadiance, false, false>(wmap[warp], wlev[warp], s, lane, slots, qb, qe, k,
                                        n_emitted, out, order, 4, r_hint);
   }
 }
