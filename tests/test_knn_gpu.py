@@ -229,3 +229,34 @@ def test_page_locked_host_buffers(ctx):
     torch.cuda.synchronize()
     np.testing.assert_array_equal(dout[1:].cpu().numpy().reshape(n, 3), want)
     assert dout[0].item() == 0.0
+
+
+def test_ragged_query_counts_all_paths(ctx):
+    """Query counts below one work item, ending inside a group of 8 or just
+    past one: the pageable, page-locked and device paths give the same
+    radiance, equal to the FP64 recomputation on the oracle's neighbours,
+    and write nothing past the last query."""
+    import torch
+    ph = W.wall_photons(20000, 31)
+    pm = gpu_map(ctx, ph)
+    qall = W.wall_queries(80, 32)
+    for n in (1, 3, 7, 8, 9, 15, 16, 17, 23, 33, 80):
+        q = np.ascontiguousarray(qall[:n])
+        want = pm.radiance(q, 30, 20000)
+        oidx, ocnt, omd2 = O.knn(ph, q[:, :3], 30)
+        assert_radiance_close(want, O.radiance_fp64(ph, oidx, ocnt, omd2, q, 20000),
+                              what=f"n={n}")
+        hq = torch.from_numpy(q).pin_memory()
+        hout = torch.full((n + 1, 3), -7.0, dtype=torch.float32).pin_memory()
+        ctx.check(ctx.lib.pm_photonmap_radiance(ctx.handle, 0, hq.data_ptr(), n, 30, 20000,
+                                                hout.data_ptr()), "pm_photonmap_radiance")
+        np.testing.assert_array_equal(hout[:n].numpy(), want)
+        assert (hout[n].numpy() == -7.0).all()
+        dq = torch.from_numpy(q).cuda()
+        dout = torch.full((n + 1, 3), -7.0, dtype=torch.float32, device="cuda")
+        ctx.check(ctx.lib.pm_photonmap_radiance_device(ctx.handle, 0, dq.data_ptr(), n, 30,
+                                                       20000, dout.data_ptr(), None),
+                  "pm_photonmap_radiance_device")
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(dout[:n].cpu().numpy(), want)
+        assert (dout[n].cpu().numpy() == -7.0).all()
