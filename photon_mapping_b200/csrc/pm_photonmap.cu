@@ -287,8 +287,7 @@ __device__ __forceinline__ void cp_async_wait_all() {
 }
 
 struct Levels {
-  int off[kMaxLevels];
-  int cnt[kMaxLevels];
+  int2 oc[kMaxLevels];  // {offset of the level's boxes, boxes in the level}
 };
 
 enum { kStatQueries = 0, kStatCold, kStatCand, kStatLeaves, kStatNodes, kStatSelects };
@@ -671,8 +670,9 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
     const int c = node * 32 + lane;
     stat_add<S>(s, lane, kStatNodes, 1);
     bool pass = false;
-    if (c < L.cnt[cl]) {
-      const int jb = L.off[cl] + c;
+    const int2 oc = L.oc[cl];
+    if (c < oc.y) {
+      const int jb = oc.x + c;
       const float4 lo = __ldg(m.boxes + 2 * jb);
       const float4 hi = __ldg(m.boxes + 2 * jb + 1);
       pass = box_dist2(q.x, q.y, q.z, lo, hi) <= q.tau;
@@ -731,8 +731,9 @@ __device__ __forceinline__ float cold_tau(const float4* pos4, const float4* boxe
   for (int cl = nlevels - 2; cl >= 0; --cl) {
     const int c = node * 32 + lane;
     unsigned long long key = ~0ull;
-    if (c < L.cnt[cl]) {
-      const int jb = L.off[cl] + c;
+    const int2 oc = L.oc[cl];
+    if (c < oc.y) {
+      const int jb = oc.x + c;
       const float d = box_dist2(qx, qy, qz, __ldg(boxes + 2 * jb),
                                 __ldg(boxes + 2 * jb + 1));
       key = ((unsigned long long)__float_as_uint(d) << 32) | (unsigned)c;
@@ -751,7 +752,7 @@ __device__ __forceinline__ float cold_tau(const float4* pos4, const float4* boxe
   // the photons of the 32 groups sharing the nearest group's parent (a
   // compact patch of 256 Morton-adjacent photons), or more groups around
   // it when k needs them
-  const int ngroups = L.cnt[0];
+  const int ngroups = L.oc[0].y;
   const int want = min(ngroups, max(32, (k + kGroup - 1) / kGroup + 8));
   const int first =
       max(0, min(want == 32 ? (node & ~31) : node - want / 2, ngroups - want));
@@ -1037,8 +1038,7 @@ __global__ void __launch_bounds__(256, 4)
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int i = 0; i < kMaxLevels; ++i) {  // constant indices: m stays in
-      L.off[i] = m.lvl_off[i];              // the parameter bank
-      L.cnt[i] = m.lvl_cnt[i];
+      L.oc[i] = make_int2(m.lvl_off[i], m.lvl_cnt[i]);  // the parameter bank
     }
   }
   if (lane < 8) s.stat[lane] = 0;
@@ -1165,8 +1165,7 @@ __global__ void __launch_bounds__(256, 4)
         const BatchScene& bs = t.scenes[sc];
         wmap[warp] = bs.map;
         for (int i = 0; i < kMaxLevels; ++i) {
-          wlev[warp].off[i] = bs.map.lvl_off[i];
-          wlev[warp].cnt[i] = bs.map.lvl_cnt[i];
+          wlev[warp].oc[i] = make_int2(bs.map.lvl_off[i], bs.map.lvl_cnt[i]);
         }
       }
       __syncwarp();
