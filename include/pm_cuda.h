@@ -80,6 +80,8 @@ typedef struct pm_knn_stats {
   uint64_t leaves;      /* 8-photon groups scanned                           */
   uint64_t nodes;       /* inner tree nodes expanded                         */
   uint64_t selects;     /* k-th distance selections                          */
+  uint64_t walks;       /* tree walks: more than one per query when a guessed
+                           radius held fewer than k photons                  */
 } pm_knn_stats;
 
 /* Turns the kNN counters on (1) or off (0) for later launches. */

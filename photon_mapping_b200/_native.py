@@ -156,7 +156,7 @@ class Context:
     def synchronize(self) -> None:
         self.check(self.lib.pm_ctx_synchronize(self.handle), "synchronize")
 
-    STAT_FIELDS = ("queries", "cold_starts", "candidates", "leaves", "nodes", "selects")
+    STAT_FIELDS = ("queries", "cold_starts", "candidates", "leaves", "nodes", "selects", "walks")
 
     def set_stats(self, enable: bool) -> None:
         self.check(self.lib.pm_ctx_set_stats(self.handle, int(bool(enable))), "pm_ctx_set_stats")

@@ -290,7 +290,7 @@ struct Levels {
   int2 oc[kMaxLevels];  // {offset of the level's boxes, boxes in the level}
 };
 
-enum { kStatQueries = 0, kStatCold, kStatCand, kStatLeaves, kStatNodes, kStatSelects };
+enum { kStatQueries = 0, kStatCold, kStatCand, kStatLeaves, kStatNodes, kStatSelects, kStatWalks };
 
 // Counters are compiled in only for the kernels launched with statistics.
 template <bool S, int C>
@@ -653,6 +653,7 @@ template <int C, bool S>
 __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
                                         Query& q, WarpBuf<C>& s, int lane) {
   q.cnt = 0;
+  stat_add<S>(s, lane, kStatWalks, 1);
   if (m.nlevels == 1) {  // a single 8-photon group
     scan_range<C, S>(m, q, s, lane, 0, m.n);
     return;
@@ -1059,7 +1060,7 @@ __global__ void __launch_bounds__(256, 4)
                           r_hint);
     if (S) {
       __syncwarp();
-      if (lane < 6) {
+      if (lane < 7) {
         atomicAdd(out.stats + lane, (unsigned long long)s.stat[lane]);
         s.stat[lane] = 0;
       }

@@ -260,3 +260,27 @@ def test_ragged_query_counts_all_paths(ctx):
         torch.cuda.synchronize()
         np.testing.assert_array_equal(dout[:n].cpu().numpy(), want)
         assert (dout[n].cpu().numpy() == -7.0).all()
+
+
+def test_stats_counters(ctx):
+    """pm_ctx_set_stats / pm_ctx_get_stats: per-query counters of the
+    radiance kernel are consistent and reset on request; disabled counters
+    stay at zero."""
+    ph = W.wall_photons(50000, 41)
+    pm = gpu_map(ctx, ph)
+    q = W.wall_queries(3000, 42)
+    ctx.get_stats(reset=True)
+    ctx.set_stats(True)
+    try:
+        pm.radiance(q, 50, 50000)
+        st = ctx.get_stats(reset=True)
+    finally:
+        ctx.set_stats(False)
+    assert st["queries"] == q.shape[0]
+    assert st["walks"] >= st["queries"]
+    assert st["candidates"] >= 50 * st["queries"]
+    assert st["leaves"] > 0 and st["nodes"] > 0
+    assert 0 < st["cold_starts"] <= st["queries"]
+    assert st["selects"] >= 1
+    pm.radiance(q, 50, 50000)
+    assert all(v == 0 for v in ctx.get_stats().values())
