@@ -264,6 +264,54 @@ def cpu_render_rate(mesh, pmi, c) -> dict | None:
                        f"-fopenmp) over the same photon maps, {secs:.1f} s")}
 
 
+def knn_uniform_cube(ctx, d_q, nq: int, flush, stream, steps: int, warmup: int, dev) -> dict:
+    """The kNN radiance kernel on a second photon set: 1,000,000 photons
+    uniform in the unit cube (a volume, where the traced map lies on
+    surfaces), answering the same primary-hit queries at k = 100, timed like
+    the headline step (CUDA events on the launching stream, L2 flushed)."""
+    import torch
+    from photon_mapping_b200 import PhotonMap
+    from photon_mapping_b200 import _native as N
+    from photon_mapping_b200 import workloads as W
+    n = 1_000_000
+    pm = PhotonMap(ctx, map_id=N.PM_MAP_CAUSTICS)
+    pm.setPhotons(W.uniform_photons(n, seed=0))
+    pm.build()
+    out = torch.empty((nq, 3), dtype=torch.float32, device=dev)
+
+    def step():
+        ctx.check(ctx.lib.pm_photonmap_radiance_device(
+            ctx.handle, N.PM_MAP_CAUSTICS, d_q.data_ptr(), nq, K_NEAREST, n, out.data_ptr(),
+            stream.cuda_stream), "pm_photonmap_radiance_device")
+
+    for _ in range(max(warmup, 0)):
+        flush.zero_()
+        step()
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    torch.cuda.synchronize(dev)
+    for e0, e1 in evs:
+        flush.zero_()
+        e0.record(stream)
+        step()
+        e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = sum(e0.elapsed_time(e1) for e0, e1 in evs) / len(evs)
+    ctx.set_stats(True)
+    step()
+    torch.cuda.synchronize(dev)
+    st = ctx.get_stats(reset=True)
+    ctx.set_stats(False)
+    peak, _ = measured_peak_hbm()
+    achieved = nq * BYTES_PER_QUERY / (ms / 1e3) / 1e9
+    return {
+        "workload": "1000000 photons uniform in the unit cube, the same primary-hit queries, k=100",
+        "photons": n, "k": K_NEAREST, "queries": nq, "ms_per_step": ms,
+        "queries_per_s": nq / (ms / 1e3), "achieved_gbs": achieved, "frac": achieved / peak,
+        "knn_per_query": {k2: v / max(st["queries"], 1) for k2, v in st.items() if k2 != "queries"},
+    }
+
+
 def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
     """Camera samples per second of pm_render (host API, wall clock) for
     the configs above, photon maps traced beforehand; beside each, the
@@ -551,6 +599,7 @@ def run_ours(args) -> None:
     st = ctx.get_stats(reset=True)
     ctx.set_stats(False)
     per_q = {k2: v / max(st["queries"], 1) for k2, v in st.items() if k2 != "queries"}
+    uniform = knn_uniform_cube(ctx, d_q, nq, flush, stream, args.steps, args.warmup, dev)
 
     render = {} if args.no_render else render_rates(
         ctx, sc, mesh, camera, dev, cpu=(rank == 0 and world == 1 and not args.no_cpu_baseline))
@@ -597,6 +646,7 @@ def run_ours(args) -> None:
                 "d2h_bytes_per_step": int(nq * 3 * 4)},
         "gpu_launches": args.steps,
         "knn_per_query": per_q,
+        "knn_uniform_cube": uniform,
         "photon_trace": {"emitted": N_EMIT, "stored": trace_stats["stored"],
                          "seconds": trace_s, "photons_per_s": N_EMIT / trace_s,
                          "includes": "emission, tracing, ordering and the map build"},
