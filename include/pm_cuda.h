@@ -158,9 +158,12 @@ int pm_photonmap_radiance_device(pm_ctx* ctx, int map, const void* d_queries,
  * device memory of the current device; the call enqueues the map build
  * and the queries on `stream` (NULL: legacy default stream) and returns.
  * Intermediate buffers live in one static device array (about 3.9 MiB per
- * GPU that loads the library, kept until exit). The first call on a device
- * looks that array's address up (cudaGetSymbolAddress) and should come
- * before any stream capture. Calls share the array: calls that overlap on
+ * GPU that loads the library, kept until exit). Every call looks that
+ * array's address up (cudaGetSymbolAddress) in the CUDA context current at
+ * the call, so a non-primary context or a context made after
+ * cudaDeviceReset gets its own address; the first call in a context loads
+ * the library's device code and should come before any stream capture.
+ * Calls share the array: calls that overlap on
  * the GPU race and must be serialised by the caller. Larger photon sets
  * are rejected with PM_ERR_INVALID_ARGUMENT. */
 #define PM_NOALLOC_MAX_PHOTONS 65536

@@ -10,9 +10,13 @@
 // __device__ array sized for kNoAllocMaxPhotons photons (about 3.9 MiB,
 // held by every GPU that loads the library until the process exits).
 //
-// Set-up: the first call on a device looks the array's device address up
-// with cudaGetSymbolAddress (once per device, with that device current) and
-// caches it; that first call should come before any stream capture.
+// Set-up: every call looks the array's device address up with
+// cudaGetSymbolAddress in the CUDA context current at the call. The address
+// belongs to that context (a plug-in may run in a context that is not the
+// device's primary one, and cudaDeviceReset makes a new one), so it is not
+// cached across calls; the lookup is cheap once the library's module is
+// loaded in the context. The first call in a context loads that module and
+// should come before any stream capture.
 // Every call reuses the same array: calls that overlap on the GPU (on two
 // streams, or from two host threads) race on it and must be serialised by
 // the caller. Words that must start at zero (the box of the photon set, the
@@ -20,8 +24,6 @@
 #include "../../include/pm_cuda.h"
 #include "pm_photonmap.cuh"
 #include "pm_sort.cuh"
-
-#include <mutex>
 
 namespace pm {
 
@@ -53,23 +55,15 @@ constexpr size_t kNaBytes = kNaPos4 + kNaThr4 + kNaWi2 + kNaBoxes + kNaSort + kN
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNaBytes];
 
-// Device address of g_noalloc_scratch per device, looked up once.
-static std::mutex g_noalloc_mu;
-static void* g_noalloc_ptr[64] = {};
-
-static int noalloc_scratch(int device, unsigned char** out) {
-  if (device < 0 || device >= 64) return PM_ERR_INVALID_ARGUMENT;
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (!g_noalloc_ptr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      cudaGetLastError();
-      return PM_ERR_CUDA;
-    }
-    g_noalloc_ptr[device] = p;
+// Device address of g_noalloc_scratch in the context current at the call.
+static int noalloc_scratch(unsigned char** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p) {
+    cudaGetLastError();
+    return PM_ERR_CUDA;
   }
-  *out = (unsigned char*)g_noalloc_ptr[device];
+  *out = (unsigned char*)p;
   return PM_OK;
 }
 
@@ -96,7 +90,7 @@ extern "C" int pm_photonmap_radiance_noalloc(const float* d_photons,
     return PM_ERR_CUDA;
   }
   unsigned char* base = nullptr;
-  int s = noalloc_scratch(device, &base);
+  int s = noalloc_scratch(&base);
   if (s != PM_OK) return s;
   int num_sms = 148;
   cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, device);

@@ -1,6 +1,7 @@
 """Compiles C++ programs against the drop-in headers and libpm_cuda.so."""
 from __future__ import annotations
 
+import os
 import subprocess
 from pathlib import Path
 
@@ -8,6 +9,13 @@ ROOT = Path(__file__).resolve().parents[1]
 DROPIN = ROOT / "photon_mapping_b200" / "cpp" / "include"
 LIBDIR = ROOT / "photon_mapping_b200" / "_lib"
 CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+
+
+def reference_dir() -> Path:
+    """The reference tree: PM_REFERENCE_DIR when set, else the directory
+    `reference` beside the repository root (as in oracle/Makefile)."""
+    env = os.environ.get("PM_REFERENCE_DIR")
+    return Path(env) if env else ROOT.parent / "reference"
 
 
 def compile_dropin(src: Path, out: Path, include=DROPIN) -> None:

@@ -8,9 +8,9 @@ from pathlib import Path
 
 import pytest
 
-from tests.dropin_build import ROOT, compile_dropin, CXX
+from tests.dropin_build import ROOT, compile_dropin, CXX, reference_dir
 
-REF = Path("/root/reference")
+REF = reference_dir()
 needs_ref = pytest.mark.skipif(not (REF / "include" / "camera.h").exists(),
                                reason="reference tree not present")
 

@@ -4,14 +4,13 @@ It serves callers that cannot call cudaMalloc (a plug-in whose host
 application owns all device memory, a real-time loop that cannot take the
 synchronisation an allocation implies): the caller hands over device
 buffers and the library keeps its intermediates in a static device array.
-This test calls it through the C ABI twice in a row, on different photon
-sets, and checks each result against the context-based
-pm_photonmap_radiance on the same inputs. It lives in its own file so that
-pytest collects it last; it also passes alone in a fresh process.
+These tests call it through the C ABI, several times in a row on different
+inputs, and check each result against the context-based
+pm_photonmap_radiance on the same inputs: the same kernels run on the same
+photon set, so the results must be identical, bit for bit. The file is
+collected last; it also passes alone in a fresh process.
 """
 from __future__ import annotations
-
-import ctypes as C
 
 import numpy as np
 import pytest
@@ -21,8 +20,6 @@ from photon_mapping_b200 import _native as N
 from photon_mapping_b200 import workloads as W
 
 pytestmark = pytest.mark.gpu
-
-RTOL = 1e-5  # the radiance tolerance of the other tests
 
 
 def noalloc_call(lib, photons_t, queries_t, out_t, k, n_emitted, stream):
@@ -38,12 +35,20 @@ def test_noalloc_matches_context_entry_point():
     lib = N.load()
     stream = torch.cuda.current_stream(dev).cuda_stream
     cases = [
+        # the largest photon set accepted
         (W.wall_photons(N.PM_NOALLOC_MAX_PHOTONS, 31), W.wall_queries(6000, 32), 100, 250000),
+        # a second, smaller set right after it (the array keeps the last contents)
         (W.wall_photons(9000, 33), W.wall_queries(3000, 34), 40, 12345),
+        # a query count that ends inside a group of 8
+        (W.wall_photons(5000, 35), W.wall_queries(13, 36), 50, 5000),
+        # k above the photon count: every photon is a neighbour
+        (W.wall_photons(37, 37), W.wall_queries(100, 38), 64, 37),
+        # no photons at all: zero radiance
+        (np.zeros((0, 9), np.float32), W.wall_queries(21, 39), 10, 1000),
     ]
     with Context(0) as ctx:
-        for ph, q, k, n_emit in cases:   # two calls in a row, different inputs
-            ph_t = torch.from_numpy(ph).to(dev)
+        for ph, q, k, n_emit in cases:
+            ph_t = torch.from_numpy(np.ascontiguousarray(ph)).to(dev)
             q_t = torch.from_numpy(q).to(dev)
             out_t = torch.full((q.shape[0], 3), float("nan"), device=dev)
             st = noalloc_call(lib, ph_t, q_t, out_t, k, n_emit, stream)
@@ -54,7 +59,9 @@ def test_noalloc_matches_context_entry_point():
             pm.setPhotons(ph)
             pm.build()
             want = pm.radiance(q, k, n_emit)
-            np.testing.assert_allclose(got, want, rtol=RTOL, atol=0)
+            np.testing.assert_array_equal(got, want, err_msg=f"{ph.shape[0]} photons, k={k}")
+            if ph.shape[0] == 0:
+                assert (got == 0).all()
 
 
 def test_noalloc_rejects_oversized_photon_sets():
