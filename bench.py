@@ -40,7 +40,10 @@ TRACE_SEED = 1
 MAX_DEPTH = 100
 IMAGE_W = IMAGE_H = 512
 SPP = 4                     # the query frame: primary hits of 512x512x4 spp
-BYTES_PER_QUERY = 36 * K_NEAREST + 24  # k photons x 36 B + position in + RGB out
+# algorithmic bytes per query: k photons x 36 B (position, throughput, wi),
+# the 48-B radiance query record in (position, wo, shading normal, albedo)
+# and the 12-B RGB out
+BYTES_PER_QUERY = 36 * K_NEAREST + 48 + 12
 METRIC = "kNN radiance queries/s at 1M photons k=100"
 CPU_SAMPLE_QUERIES = 40000
 
@@ -310,6 +313,33 @@ def knn_uniform_cube(ctx, d_q, nq: int, flush, stream, steps: int, warmup: int, 
         "queries_per_s": nq / (ms / 1e3), "achieved_gbs": achieved, "frac": achieved / peak,
         "knn_per_query": {k2: v / max(st["queries"], 1) for k2, v in st.items() if k2 != "queries"},
     }
+
+
+def workload_parity(ctx, photons, queries, rgb) -> dict:
+    """Exactness of the timed workload on a sample of its queries (outside
+    the timed region): the neighbour lists of the same query stream (every
+    query, in pixel order, through pm_photonmap_knn) against the oracle's
+    brute-force exact kNN, and the timed steps' radiance `rgb` against the
+    FP64 recomputation on the oracle's neighbour sets."""
+    from oracle import oracle as O
+    from photon_mapping_b200 import PM_MAP_GLOBAL, PhotonMap
+    from photon_mapping_b200 import workloads as W
+    pm = PhotonMap(ctx, PM_MAP_GLOBAL)
+    idx, cnt, md2 = pm.query_knn(queries[:, :3], K_NEAREST)
+    s = W.parity_sample(queries.shape[0])
+    t0 = time.perf_counter()
+    oidx, ocnt, omd2 = O.knn(photons, queries[s, :3], K_NEAREST)
+    secs = time.perf_counter() - t0
+    mism = int(((idx[s] != oidx).any(axis=1) | (md2[s] != omd2) | (cnt[s] != ocnt)).sum())
+    want = O.radiance_fp64(photons, oidx, ocnt, omd2, queries[s], N_EMIT)
+    err = np.abs(rgb[s] - want) / np.maximum(np.abs(want), 1e-30)
+    return {"sample": int(s.size), "mismatches": mism, "max_rel_err": float(err.max()),
+            "tolerance": 1e-5,
+            "oracle": ("brute-force exact kNN over every photon (FP32 distance in the reference's "
+                       "order, ties to the smaller index), radiance recomputed in FP64"),
+            "sample_kind": ("runs of 64 consecutive queries from work-item starts, the last 64, "
+                            "first queries of 512 work items, 1024 random"),
+            "oracle_s": secs}
 
 
 def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
@@ -592,6 +622,10 @@ def run_ours(args) -> None:
     e2e_value = world * nq / e2e_s
     clk = clocks.stop()  # sampled over the timed steps and the e2e steps
 
+    parity = None
+    if rank == 0:
+        parity = workload_parity(ctx, photons, queries, d_out.cpu().numpy())
+
     # one more (untimed) pass with the kernel's counters on
     ctx.set_stats(True)
     step()
@@ -645,6 +679,7 @@ def run_ours(args) -> None:
                 "h2d_bytes_per_step": int(queries.nbytes),
                 "d2h_bytes_per_step": int(nq * 3 * 4)},
         "gpu_launches": args.steps,
+        "parity": parity,
         "knn_per_query": per_q,
         "knn_uniform_cube": uniform,
         "photon_trace": {"emitted": N_EMIT, "stored": trace_stats["stored"],

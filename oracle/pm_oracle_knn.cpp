@@ -49,29 +49,40 @@ extern "C" {
 // Output per query, like KdTree::searchKNearest (photon_map.h:166-183):
 // indices in heap-pop order (largest (dist2, index) first), padded with -1,
 // the number returned and maxDist2 (largest kept dist2, 0 when none).
-// Photons whose distance is NaN are never returned.
+// Photons whose distance is NaN are never returned. Every photon is tested;
+// a max-heap of the k smallest (dist2, index) pairs seen so far (the
+// bounded queue of photon_map.h:120-126) keeps the scan linear.
 void orc_knn(const float* photons, int64_t n, const float* queries,
              int64_t nq, int k, int32_t* out_idx, int32_t* out_cnt,
              float* out_maxd2) {
 #pragma omp parallel
   {
-    std::vector<Cand> c;
-    c.reserve((size_t)n);
-#pragma omp for schedule(dynamic, 16)
+    std::vector<Cand> h;
+    h.reserve((size_t)k + 1);
+#pragma omp for schedule(dynamic, 4)
     for (int64_t qi = 0; qi < nq; ++qi) {
       const float* q = queries + 3 * qi;
-      c.clear();
+      h.clear();
       for (int64_t i = 0; i < n; ++i) {
         const float d2 = distance2(q, photons + 9 * i + 3);
-        if (!std::isnan(d2)) c.push_back({d2, (int32_t)i});
+        if (std::isnan(d2)) continue;
+        const Cand c{d2, (int32_t)i};
+        if ((int)h.size() < k) {
+          h.push_back(c);
+          std::push_heap(h.begin(), h.end(), pair_less);
+        } else if (pair_less(c, h.front())) {
+          std::pop_heap(h.begin(), h.end(), pair_less);
+          h.back() = c;
+          std::push_heap(h.begin(), h.end(), pair_less);
+        }
       }
-      const size_t kk = std::min<size_t>((size_t)k, c.size());
-      std::partial_sort(c.begin(), c.begin() + kk, c.end(), pair_less);
+      std::sort_heap(h.begin(), h.end(), pair_less);  // ascending
+      const size_t kk = h.size();
       int32_t* row = out_idx + qi * (int64_t)k;
       float maxd2 = 0.f;
       for (size_t r = 0; r < kk; ++r) {
-        row[r] = c[kk - 1 - r].idx;  // descending
-        maxd2 = std::max(maxd2, c[r].d2);
+        row[r] = h[kk - 1 - r].idx;  // descending
+        maxd2 = std::max(maxd2, h[r].d2);
       }
       for (size_t r = kk; r < (size_t)k; ++r) row[r] = -1;
       out_cnt[qi] = (int32_t)kk;

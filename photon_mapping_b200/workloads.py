@@ -254,3 +254,55 @@ def rays8(o, d, tmin: float = 1e-5):
     r[:, 0:3], r[:, 3], r[:, 4:7] = o, tmin, d
     r[:, 7] = np.finfo(np.float32).max
     return r
+
+
+def traced_cornell_knn_workload(ctx, n_emit: int = 1_000_000, seed: int = 1, width: int = 512,
+                                height: int = 512, spp: int = 4, max_depth: int = 100):
+    """The kNN radiance workload of the benchmark: the global photon map
+    traced on the device from `n_emit` photons emitted in the procedural
+    Cornell box (seed 0 scene, trace seed `seed`; PhotonMapping::build,
+    integrator.h:393-474, without final gathering), and one
+    pm_radiance_query per primary hit of a width x height x spp frame on a
+    non-emitting Lambert face, in pixel order (sample-minor).
+
+    Leaves the scene and the traced map on `ctx` (map PM_MAP_GLOBAL).
+    Returns (scene, mesh, camera, photons (n, 9), queries (nq, 12), trace
+    statistics)."""
+    from . import scene as S
+    from .camera import Camera
+    from .integrator import PhotonMapping
+    mesh = S.cornell_box(0)
+    camera = Camera(S.CAMERA["position"], S.CAMERA["forward"], S.CAMERA["fov"])
+    sc = S.Scene(ctx)
+    sc.setMesh(mesh)
+    sc.build()
+    pmi = PhotonMapping(n_emit, 100, 1.0, 100, 0, max_depth, ctx=ctx)
+    stats = pmi.build(sc, seed=seed)["global"]
+    photons = pmi.global_map.photons()
+    o, d = camera_rays(camera, width, height, spp)
+    queries = hit_queries(mesh, o, d, sc.intersect(o, d))
+    return sc, mesh, camera, photons, queries, stats
+
+
+def parity_sample(nq: int, seed: int = 0, runs: int = 40, run_len: int = 64, starts: int = 512,
+                  singles: int = 1024) -> np.ndarray:
+    """Indices of a sample of a query stream of length nq for exactness
+    checks against brute force: `runs` runs of `run_len` consecutive
+    queries beginning at multiples of 16 (the first query of a run of the
+    kNN kernel's work items, then its warm successors), the last run_len
+    queries (the short work items at the end of a launch), the first query
+    of `starts` work items, and `singles` queries drawn at random. Sorted,
+    without repeats."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    if nq > 0:
+        hi = max(nq - run_len, 0)
+        for b in np.linspace(0, hi, runs).astype(np.int64):
+            b = (b // 16) * 16
+            parts.append(np.arange(b, min(b + run_len, nq)))
+        parts.append(np.arange(max(nq - run_len, 0), nq))
+        parts.append((rng.integers(0, max(nq // 16, 1), starts) * 16).clip(0, nq - 1))
+        parts.append(rng.integers(0, nq, singles))
+    if not parts:
+        return np.zeros(0, np.int64)
+    return np.unique(np.concatenate(parts)).astype(np.int64)
