@@ -69,7 +69,7 @@ def test_deep_tree_intersections_exact_with_the_default_stack(ctx):
     want = O.OracleScene(mesh).intersect(r)
     np.testing.assert_array_equal(got["prim"], want[:, 3].view(np.int32))
     hit = got["prim"] >= 0
-    assert hit.mean() > 0.2
+    assert hit.sum() > 20          # thin triangles: few rays hit one
     np.testing.assert_array_equal(got["t"][hit], want[hit, 0])
 
 
