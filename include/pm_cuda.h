@@ -81,7 +81,9 @@ typedef struct pm_knn_stats {
   uint64_t nodes;       /* inner tree nodes expanded                         */
   uint64_t selects;     /* k-th distance selections                          */
   uint64_t walks;       /* tree walks: more than one per query when a guessed
-                           radius held fewer than k photons                  */
+                           radius held fewer than k photons; one per
+                           neighbourhood pool                                */
+  uint64_t pool_queries; /* queries answered from a neighbourhood pool       */
 } pm_knn_stats;
 
 /* Turns the kNN counters on (1) or off (0) for later launches. */
@@ -89,6 +91,14 @@ int pm_ctx_set_stats(pm_ctx* ctx, int enable);
 /* Copies the counters (waits for the context's stream); reset != 0 zeroes
  * them afterwards. */
 int pm_ctx_get_stats(pm_ctx* ctx, pm_knn_stats* out, int reset);
+
+/* Neighbourhood pools of the kNN kernels (no reference counterpart; on by
+ * default): for k <= 128 a group of nearby queries shares one tree walk
+ * that collects the photons around them, and each member selects its k
+ * nearest from that pool. 0 turns them off (every query walks the tree on
+ * its own), 1 back on. Results are identical either way; only the speed
+ * changes. */
+int pm_ctx_set_knn_pool(pm_ctx* ctx, int enable);
 
 /* ---------------------------------------------------------- photon map */
 /* Replaces PhotonMap::setPhotons + PhotonMap::build

@@ -206,6 +206,13 @@ int pm_ctx_set_stats(pm_ctx* c, int enable) {
   return PM_OK;
 }
 
+int pm_ctx_set_knn_pool(pm_ctx* c, int enable) {
+  PM_CHECK_CTX(c);
+  std::lock_guard<std::mutex> lk(c->mu);
+  c->knn_pool = enable != 0;
+  return PM_OK;
+}
+
 int pm_ctx_get_stats(pm_ctx* c, pm_knn_stats* out, int reset) {
   PM_CHECK_CTX(c);
   if (!out) return PM_ERR_INVALID_ARGUMENT;
@@ -333,7 +340,7 @@ int pm_photonmap_knn(pm_ctx* c, int map, const float* queries, int64_t nq,
   o.count = m_cnt ? m_cnt : (int32_t*)((char*)c->q_out.ptr + ib);
   o.maxd2 = m_md2 ? m_md2 : (float*)((char*)c->q_out.ptr + ib + cb);
   e = knn_launch(map_view(dm), c->q_in.ptr, nq, k, kModeKnn, 0.f, o,
-                 c->next_counter(), c->num_sms, st);
+                 c->next_counter(), c->num_sms, st, nullptr, 3, c->knn_pool);
   if (e != cudaSuccess) return cuda_status(c, e, "knn launch");
   if ((!m_idx && (e = cudaMemcpyAsync(out_idx, o.idx, ib, cudaMemcpyDeviceToHost, st))) ||
       (!m_cnt && (e = cudaMemcpyAsync(out_count, o.count, cb, cudaMemcpyDeviceToHost, st))) ||
@@ -380,7 +387,8 @@ int pm_photonmap_radiance(pm_ctx* c, int map, const pm_radiance_query* q,
   o.stats = c->stats_ptr();
   o.rgb = mapped_out ? mapped_out : (float*)c->q_out.ptr;
   e = knn_launch(map_view(dm), d_q, nq, k, kModeRadiance,
-                 (float)n_emitted, o, c->next_counter(), c->num_sms, st);
+                 (float)n_emitted, o, c->next_counter(), c->num_sms, st, nullptr, 3,
+                 c->knn_pool);
   if (e != cudaSuccess) return cuda_status(c, e, "radiance launch");
   if (!mapped_out) {
     e = cudaMemcpyAsync(out_rgb, o.rgb, ob, cudaMemcpyDeviceToHost, st);
@@ -411,7 +419,7 @@ int pm_photonmap_radiance_device(pm_ctx* c, int map, const void* d_queries,
   o.rgb = (float*)d_out_rgb;
   cudaError_t e = knn_launch(map_view(dm), d_queries, nq, k, kModeRadiance,
                              (float)n_emitted, o, c->next_counter(),
-                             c->num_sms, as_stream(stream));
+                             c->num_sms, as_stream(stream), nullptr, 3, c->knn_pool);
   return cuda_status(c, e, "radiance launch");
 }
 

@@ -123,6 +123,7 @@ struct pm_ctx {
   pm::DevBuf stats;        // pm_knn_stats counters (device)
   pm::DiffState diff;      // differentiable render
   bool stats_on = false;
+  bool knn_pool = true;    // neighbourhood pools in the kNN kernels
   unsigned long long* stats_ptr() {
     return stats_on ? (unsigned long long*)stats.ptr : nullptr;
   }

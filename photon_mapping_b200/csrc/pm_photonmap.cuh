@@ -53,7 +53,7 @@ struct KnnOut {
   int32_t* idx;        // knn mode: k per query
   int32_t* count;      // knn mode
   float* maxd2;        // knn mode
-  unsigned long long* stats;  // 6 counters (pm_knn_stats) or null
+  unsigned long long* stats;  // the pm_knn_stats counters or null
   const float* adj_in;  // adjoint mode: d loss / d estimate, 3 floats per record
   float4* photon_adj;   // adjoint mode: d loss / d throughput per photon
                         // (index order, .xyz), accumulated atomically
@@ -67,11 +67,13 @@ struct KnnOut {
 //   adjoint mode:  the records of radiance mode; the neighbours of record r
 //                  receive adj_in[3r .. 3r+3) times d estimate / d
 //                  throughput in photon_adj
-// `counter` is one device word of scratch (reset by this call).
+// `counter` is one device word of scratch (reset by this call). `pool`
+// lets the kernel answer groups of nearby queries from one shared
+// neighbourhood walk (k <= 128; the results are the same either way).
 cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                        int k, int mode, float n_emitted, KnnOut out,
                        unsigned long long* counter, int num_sms,
                        cudaStream_t st, const uint32_t* order = nullptr,
-                       int stride4 = 3);
+                       int stride4 = 3, bool pool = true);
 
 }  // namespace pm

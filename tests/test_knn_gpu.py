@@ -284,3 +284,64 @@ def test_stats_counters(ctx):
     assert st["selects"] >= 1
     pm.radiance(q, 50, 50000)
     assert all(v == 0 for v in ctx.get_stats().values())
+
+
+@pytest.mark.parametrize("k", [1, 16, 50, 100, 128])
+def test_pools_change_nothing(ctx, k):
+    """Neighbourhood pools (pm_ctx_set_knn_pool) answer most queries of a
+    coherent stream, and give the same lists, distances and radiance, bit
+    for bit, as the per-query search; both equal brute force."""
+    ph = W.wall_photons(120000, 300 + k)
+    q = W.wall_queries(6000, 400 + k)
+    q = q[np.lexsort((q[:, 2], q[:, 1], q[:, 0]))]  # spatially coherent order
+    pm = gpu_map(ctx, ph)
+    results = {}
+    for pool in (True, False):
+        ctx.set_knn_pool(pool)
+        ctx.get_stats(reset=True)
+        ctx.set_stats(True)
+        try:
+            lists = pm.query_knn(q[:, :3], k)
+            rad = pm.radiance(q, k, 120000)
+            st = ctx.get_stats(reset=True)
+        finally:
+            ctx.set_stats(False)
+            ctx.set_knn_pool(True)
+        results[pool] = (lists, rad, st)
+    (a, ra, sa), (b, rb, sb) = results[True], results[False]
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(ra, rb)
+    assert sb["pool_queries"] == 0
+    assert sa["pool_queries"] > 0.8 * sa["queries"], sa
+    sample = np.arange(0, q.shape[0], 7)
+    oidx, ocnt, omd2 = O.knn(ph, q[sample, :3], k)
+    np.testing.assert_array_equal(a[0][sample], oidx)
+    np.testing.assert_array_equal(a[2][sample], omd2)
+    assert_radiance_close(ra[sample], O.radiance_fp64(ph, oidx, ocnt, omd2, q[sample], 120000),
+                          what=f"k={k}")
+
+
+def test_pools_with_ties_and_duplicates(ctx):
+    """Photons on a lattice (many equal distances) and repeated photons:
+    pooled answers equal the per-query search and brute force."""
+    lat = W.lattice_photons(12, 0.125, seed=4)
+    dup = np.repeat(W.wall_photons(3000, 5), 3, axis=0)
+    for ph in (lat, dup):
+        pm = gpu_map(ctx, ph)
+        rng = np.random.default_rng(6)
+        q = ph[rng.choice(ph.shape[0], 2000), 3:6].copy()
+        q[1::2] += rng.normal(scale=0.01, size=q[1::2].shape).astype(np.float32)
+        q = q[np.lexsort((q[:, 2], q[:, 1], q[:, 0]))]
+        got = {}
+        for pool in (True, False):
+            ctx.set_knn_pool(pool)
+            try:
+                got[pool] = pm.query_knn(q, 40)
+            finally:
+                ctx.set_knn_pool(True)
+        for x, y in zip(got[True], got[False]):
+            np.testing.assert_array_equal(x, y)
+        want = O.knn(ph, q, 40)
+        for x, y in zip(got[True], want):
+            np.testing.assert_array_equal(x, y)
