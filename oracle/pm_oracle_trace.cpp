@@ -87,33 +87,31 @@ static inline uint64_t splitmix64(uint64_t x) {
   return x ^ (x >> 31);
 }
 
-// sin/cos of a float angle: reduction by pi/2 and Taylor series in double.
-static inline void sincos_d(float xf, float& s, float& c) {
-  const double x = (double)xf;
-  const double q = std::rint(x * 0.63661977236758134308);
-  const double r = x - q * 1.5707963267948966192;
-  const double r2 = r * r;
-  static const double sin_inv_fact[9] = {
-      1.0 / 355687428096000.0, 1.0 / 1307674368000.0, 1.0 / 6227020800.0,
-      1.0 / 39916800.0,        1.0 / 362880.0,        1.0 / 5040.0,
-      1.0 / 120.0,             1.0 / 6.0,             1.0};
-  static const double cos_inv_fact[9] = {
-      1.0 / 6402373705728000.0, 1.0 / 20922789888000.0, 1.0 / 87178291200.0,
-      1.0 / 479001600.0,        1.0 / 3628800.0,        1.0 / 40320.0,
-      1.0 / 720.0,              1.0 / 24.0,             1.0 / 2.0};
-  double ps = sin_inv_fact[0];
-  for (int i = 1; i < 9; ++i) ps = ps * -r2 + sin_inv_fact[i];
-  const double sr = r * ps;
-  double pc = cos_inv_fact[0];
-  for (int i = 1; i < 9; ++i) pc = pc * -r2 + cos_inv_fact[i];
-  const double cr = 1.0 - r2 * pc;
+// sin/cos of a float angle |x| <= 8 in float arithmetic, one rounding per
+// operation (built with -ffp-contract=off): Cody-Waite reduction by pi/2
+// split in three floats (21 + 21 + 24 significant bits), Taylor
+// polynomials on |r| <= pi/4 (sin to r^9, cos to r^10) in Horner form with
+// the coefficients 1/n! rounded to float, quadrant q mod 4.
+static inline void sincos_f(float x, float& s, float& c) {
+  const float q = std::rint(x * 0x1.45f306p-1f);
+  float r = x - q * 0x1.921fbp+0f;
+  r = r - q * 0x1.5110bp-22f;
+  r = r - q * 0x1.184698p-44f;
+  const float r2 = r * r;
+  float ps = 1.0f / 362880.0f;
+  ps = ps * r2 + -1.0f / 5040.0f;
+  ps = ps * r2 + 1.0f / 120.0f;
+  ps = ps * r2 + -1.0f / 6.0f;
+  const float sr = r + (r * r2) * ps;
+  float pc = -1.0f / 3628800.0f;
+  pc = pc * r2 + 1.0f / 40320.0f;
+  pc = pc * r2 + -1.0f / 720.0f;
+  pc = pc * r2 + 1.0f / 24.0f;
+  pc = pc * r2 + -0.5f;
+  const float cr = 1.0f + r2 * pc;
   const int quad = ((int)q) & 3;
-  double sd = sr, cd = cr;
-  if (quad == 1) { sd = cr; cd = -sr; }
-  else if (quad == 2) { sd = -sr; cd = -cr; }
-  else if (quad == 3) { sd = -cr; cd = sr; }
-  s = (float)sd;
-  c = (float)cd;
+  s = quad == 0 ? sr : quad == 1 ? cr : quad == 2 ? -sr : -cr;
+  c = quad == 0 ? cr : quad == 1 ? -sr : quad == 2 ? -cr : sr;
 }
 
 static inline V cos_hemisphere(float u0, float u1, float& pdf) {
@@ -121,7 +119,7 @@ static inline V cos_hemisphere(float u0, float u1, float& pdf) {
   const float st = std::sqrt(u0);
   const float phi = PI_MUL_2 * u1;
   float sp, cp;
-  sincos_d(phi, sp, cp);
+  sincos_f(phi, sp, cp);
   pdf = PI_INV * ct;
   return mk(cp * st, ct, sp * st);
 }
@@ -407,7 +405,7 @@ int64_t orc_trace(void* h, int map, uint64_t seed, int64_t first, int64_t count,
 
 // sin and cos of n float angles with the double-precision evaluation above.
 void orc_sincos(const float* x, int64_t n, float* s, float* c) {
-  for (int64_t i = 0; i < n; ++i) sincos_d(x[i], s[i], c[i]);
+  for (int64_t i = 0; i < n; ++i) sincos_f(x[i], s[i], c[i]);
 }
 
 }  // extern "C"

@@ -65,12 +65,34 @@ def test_obj_loader_rules(tmp_path):
 
 
 def test_oracle_sincos_accuracy():
-    x = np.random.default_rng(0).uniform(0.0, 6.2832, 200000).astype(np.float32)
+    """The float sin/cos of the cosine-hemisphere draw (the oracle's copy of
+    the device's sincos_f32): within 2 float ulps of the exact value over
+    [-8, 8], and near the multiples of pi/2, where the reduction cancels."""
+    rng = np.random.default_rng(0)
+    near = (np.arange(-5, 6)[:, None] * (np.pi / 2) + np.linspace(-1e-5, 1e-5, 401)[None, :])
+    x = np.concatenate([rng.uniform(0.0, 6.2832, 200000), rng.uniform(-8, 8, 100000),
+                        near.ravel()]).astype(np.float32)
     s, c = O.sincos(x)
     xd = x.astype(np.float64)
-    # within one float ulp of the exact value
-    assert np.all(np.abs(s - np.sin(xd)) <= np.spacing(np.abs(np.sin(xd)).astype(np.float32)) + 1e-45)
-    assert np.all(np.abs(c - np.cos(xd)) <= np.spacing(np.abs(np.cos(xd)).astype(np.float32)) + 1e-45)
+    for got, want in ((s, np.sin(xd)), (c, np.cos(xd))):
+        ulp = np.spacing(np.abs(want).astype(np.float32)).astype(np.float64)
+        assert np.all(np.abs(got - want) <= 2 * ulp + 1e-45)
+    # the same formulas in numpy float32 (one rounding per operation) agree bit for bit
+    f = np.float32
+    q = np.rint(x * f(float.fromhex("0x1.45f306p-1")))
+    r = x - q * f(float.fromhex("0x1.921fbp+0"))
+    r = r - q * f(float.fromhex("0x1.5110bp-22"))
+    r = r - q * f(float.fromhex("0x1.184698p-44"))
+    r2 = r * r
+    ps = f(1 / 362880) * r2 + f(-1 / 5040)
+    ps = (ps * r2 + f(1 / 120)) * r2 + f(-1 / 6)
+    sr = r + (r * r2) * ps
+    pc = f(-1 / 3628800) * r2 + f(1 / 40320)
+    pc = ((pc * r2 + f(-1 / 720)) * r2 + f(1 / 24)) * r2 + f(-0.5)
+    cr = f(1) + r2 * pc
+    quad = q.astype(np.int32) & 3
+    np.testing.assert_array_equal(s, np.select([quad == 0, quad == 1, quad == 2], [sr, cr, -sr], -cr))
+    np.testing.assert_array_equal(c, np.select([quad == 0, quad == 1, quad == 2], [cr, -sr, -cr], sr))
 
 
 def test_oracle_intersect_basic():
