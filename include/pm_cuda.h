@@ -77,13 +77,15 @@ typedef struct pm_knn_stats {
   uint64_t queries;     /* queries answered                                  */
   uint64_t cold_starts; /* queries whose search radius was bounded afresh    */
   uint64_t candidates;  /* photons found within the search radius            */
-  uint64_t leaves;      /* 8-photon groups scanned                           */
+  uint64_t leaves;      /* 8-photon groups scanned (tree walks) and cell
+                           ranges scanned (grid searches)                    */
   uint64_t nodes;       /* inner tree nodes expanded                         */
   uint64_t selects;     /* k-th distance selections                          */
-  uint64_t walks;       /* tree walks: more than one per query when a guessed
-                           radius held fewer than k photons; one per
-                           neighbourhood pool                                */
-  uint64_t pool_queries; /* queries answered from a neighbourhood pool       */
+  uint64_t walks;       /* candidate searches (tree walks and grid searches):
+                           more than one per query when a guessed radius
+                           held fewer than k photons                         */
+  uint64_t grid_searches; /* searches that listed their candidates from the
+                           map's cell grid instead of walking the tree       */
 } pm_knn_stats;
 
 /* Turns the kNN counters on (1) or off (0) for later launches. */
@@ -92,13 +94,14 @@ int pm_ctx_set_stats(pm_ctx* ctx, int enable);
  * them afterwards. */
 int pm_ctx_get_stats(pm_ctx* ctx, pm_knn_stats* out, int reset);
 
-/* Neighbourhood pools of the kNN kernels (no reference counterpart; on by
- * default): for k <= 128 a group of nearby queries shares one tree walk
- * that collects the photons around them, and each member selects its k
- * nearest from that pool. 0 turns them off (every query walks the tree on
- * its own), 1 back on. Results are identical either way; only the speed
- * changes. */
-int pm_ctx_set_knn_pool(pm_ctx* ctx, int enable);
+/* Cell grids of the kNN searches (no reference counterpart; on by
+ * default). pm_photonmap_build also files the sorted photons by cell of a
+ * uniform grid (levels 3 to 7, 8^L cells, about 9.6 MB at 3M photons), and a
+ * search whose radius suits a level lists its candidates from the cells
+ * around the query instead of walking the box tree. 0 makes every search
+ * walk the tree, 1 restores the grid. Results are identical either way;
+ * only the speed changes. */
+int pm_ctx_set_knn_grid(pm_ctx* ctx, int enable);
 
 /* ---------------------------------------------------------- photon map */
 /* Replaces PhotonMap::setPhotons + PhotonMap::build
@@ -220,6 +223,10 @@ typedef struct pm_trace_stats {
   int64_t stored;               /* photons stored in the map             */
   uint32_t nan_throughput;      /* paths stopped on a NaN throughput     */
   uint32_t negative_throughput; /* paths stopped on a negative one       */
+  int64_t rays;                 /* closest-hit queries traced            */
+  float trace_ms;               /* device time of the tracing kernel     */
+  float build_ms;               /* device time of ordering the photons
+                                   and building the map                  */
 } pm_trace_stats;
 
 /* Replaces the photon-tracing half of PhotonMapping::build
@@ -277,6 +284,12 @@ typedef struct pm_render_stats {
                                  relative difference, over pixels and
                                  channels, between the image and the FP64
                                  sums of the same samples; 0 otherwise     */
+  int64_t rays;               /* closest-hit queries of the camera pass
+                                 (camera and specular rays, shadow rays,
+                                 gather rays)                              */
+  float camera_ms;            /* device time of the camera-pass kernels    */
+  float estimate_ms;          /* device time of listing, sorting and
+                                 answering the photon-map queries          */
 } pm_render_stats;
 
 /* The render loop of examples/main.cpp:33-70 with
@@ -454,6 +467,10 @@ int pm_batch_image(pm_batch* batch, int32_t scene, float* out_rgb);
 /* Photons stored and photon-map queries answered per scene (n_scenes each;
  * either may be NULL). */
 int pm_batch_counts(pm_batch* batch, int64_t* photons_stored, int64_t* queries);
+/* The photon map of scene s after the last step: photons_stored[s] records
+ * of 9 floats in index order, as PhotonMapping::build stores them for that
+ * scene (integrator.h:406-469; the counterpart of pm_photonmap_get_photons). */
+int pm_batch_photons(pm_batch* batch, int32_t scene, float* out_photons);
 
 #ifdef __cplusplus
 }

@@ -150,6 +150,14 @@ class BatchRenderer:
         self.check(self.lib.pm_batch_image(self.handle, int(i), out.ctypes.data), "pm_batch_image")
         return out
 
+    def photons(self, i: int) -> np.ndarray:
+        """Scene i's stored photons (n, 9) in index order, after the last step."""
+        stored, _ = self.counts()
+        out = np.empty((int(stored[i]), 9), np.float32)
+        self.check(self.lib.pm_batch_photons(self.handle, int(i), out.ctypes.data),
+                   "pm_batch_photons")
+        return out
+
     def counts(self) -> tuple[np.ndarray, np.ndarray]:
         n = len(self.scenes)
         st, q = np.zeros(n, np.int64), np.zeros(n, np.int64)

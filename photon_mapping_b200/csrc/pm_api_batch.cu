@@ -150,6 +150,7 @@ int upload_tables(pm_batch* b) {
                          sc.hi[1] > sc.lo[1] ? 1.0f / (sc.hi[1] - sc.lo[1]) : 0.f,
                          sc.hi[2] > sc.lo[2] ? 1.0f / (sc.hi[2] - sc.lo[2]) : 0.f);
     TraceArgs& ta = x.ta;
+    ta = TraceArgs{};
     ta.seed = d.seed;
     ta.n_emit = (int)d.n_photons;
     ta.max_depth = d.max_depth;
@@ -226,7 +227,8 @@ void enqueue_maps(pm_batch* b) {
                            (float*)dm.aos.ptr, b->scratch[i].ptr, b->side[i]);
       map_build_launch((const float*)dm.aos.ptr, m, (float4*)dm.pos4.ptr, (float4*)dm.thr4.ptr,
                        (float2*)dm.wi2.ptr, (float4*)dm.boxes.ptr, dm.lvl_off, dm.lvl_cnt,
-                       dm.nlevels, b->scratch[i].ptr, b->side[i]);
+                       dm.nlevels, b->scratch[i].ptr, b->side[i], (uint32_t*)dm.grid.ptr,
+                       dm.grid_lmax, dm.grid_off);
     }
   }
   for (int i = 0; i < ns; ++i) {
@@ -349,10 +351,12 @@ int plan(pm_batch* b) {
     const int64_t m = b->stored[i];
     dm.n = m;
     const int total = map_levels(m, &dm.nlevels, dm.lvl_off, dm.lvl_cnt);
+    const size_t gw = grid_words(m, &dm.grid_lmax, dm.grid_off);
     if (m > 0 &&
         ((s = dm.aos.ensure((size_t)m * 36)) || (s = dm.pos4.ensure((size_t)m * 16)) ||
          (s = dm.thr4.ensure((size_t)m * 16)) || (s = dm.wi2.ensure((size_t)m * 8)) ||
-         (s = dm.boxes.ensure((size_t)total * 32))))
+         (s = dm.boxes.ensure((size_t)total * 32)) ||
+         (gw > 0 && (s = dm.grid.ensure(gw * 4)))))
       return berr(b, s, "scene %d: photon map (%lld photons)", i, (long long)m);
     dm.built = true;
     const size_t sb = std::max(order_scratch_bytes(m), map_build_scratch_bytes(m));
@@ -672,6 +676,21 @@ int pm_batch_image(pm_batch* b, int32_t scene, float* out) {
                            cudaMemcpyDeviceToHost, b->st)) ||
       (e = cudaStreamSynchronize(b->st)))
     return bcuda(b, e, "batch image");
+  return PM_OK;
+}
+
+int pm_batch_photons(pm_batch* b, int32_t scene, float* out) {
+  if (!b) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
+  if (scene < 0 || scene >= b->n || !out) return berr(b, PM_ERR_INVALID_ARGUMENT, "scene / out");
+  cudaSetDevice(b->device);
+  const int64_t m = b->stored[scene];
+  if (m == 0) return PM_OK;
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(out, b->maps[scene].aos.ptr, (size_t)m * 36, cudaMemcpyDeviceToHost,
+                           b->st)) ||
+      (e = cudaStreamSynchronize(b->st)))
+    return bcuda(b, e, "batch photons");
   return PM_OK;
 }
 

@@ -25,7 +25,9 @@ struct DevMap {
   int nlevels = 0;
   int lvl_off[kMaxLevels] = {};
   int lvl_cnt[kMaxLevels] = {};
-  DevBuf aos, pos4, thr4, wi2, boxes;
+  int grid_lmax = 0;                  // cell grid: finest level (0: none)
+  int grid_off[kGridLevels] = {};
+  DevBuf aos, pos4, thr4, wi2, boxes, grid;
   bool built = false;
   void release() {
     aos.release();
@@ -33,6 +35,8 @@ struct DevMap {
     thr4.release();
     wi2.release();
     boxes.release();
+    grid.release();
+    grid_lmax = 0;
     built = false;
     n = 0;
   }
@@ -123,7 +127,7 @@ struct pm_ctx {
   pm::DevBuf stats;        // pm_knn_stats counters (device)
   pm::DiffState diff;      // differentiable render
   bool stats_on = false;
-  bool knn_pool = true;    // neighbourhood pools in the kNN kernels
+  bool knn_grid = true;    // cell-grid candidate lists in the kNN kernels
   unsigned long long* stats_ptr() {
     return stats_on ? (unsigned long long*)stats.ptr : nullptr;
   }

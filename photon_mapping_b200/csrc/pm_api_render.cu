@@ -65,7 +65,7 @@ int answer_queries(pm_ctx* c, const RenderArgs& a, int64_t ns, int64_t n_slots,
     e = knn_launch(map_view(c->maps[map]), a.slots, nq, map == 0 ? kg : kc,
                    slot_adj ? kModeAdjoint : kModeRadiance, (float)c->map_emitted[map], o,
                    c->next_counter(), c->num_sms, st, in_b ? vb : va, 4,
-                   c->knn_pool);
+                   c->knn_grid);
     if (e != cudaSuccess) return cuda_status(c, e, "render estimates");
   }
   return PM_OK;
@@ -157,16 +157,41 @@ extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
   a.cam_up = v3(cam->up[0], cam->up[1], cam->up[2]);
   a.focal = cam->focal_length;
   const SceneDev sv = c->scene_view();
+  a.rays = (unsigned long long*)((char*)c->r_misc.ptr + 48);
   int64_t q_tot[2] = {0, 0};
   int passes = 0;
+  // device time of the camera pass and of the estimates, summed over passes
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  for (auto& x : ev)
+    if ((e = cudaEventCreate(&x)) != cudaSuccess) {
+      for (auto& y : ev)
+        if (y) cudaEventDestroy(y);
+      return cuda_status(c, e, "render events");
+    }
+  struct EvGuard {
+    cudaEvent_t* ev;
+    ~EvGuard() {
+      for (int i = 0; i < 3; ++i) cudaEventDestroy(ev[i]);
+    }
+  } guard{ev};
+  float cam_ms = 0.f, est_ms = 0.f;
   for (int done = 0; done < p.spp; done += batch) {
     const int b = std::min(batch, p.spp - done);
     a.batch = b;
     const int64_t ns = (int64_t)npix * b;
+    cudaEventRecord(ev[0], st);
     render_camera(sv, a, st);
+    cudaEventRecord(ev[1], st);
     if ((s = answer_queries(c, a, ns, n_slots, need_caustics, p.k_global, p.k_caustics,
                             q_tot, nullptr, nullptr)) != PM_OK)
       return s;
+    cudaEventRecord(ev[2], st);
+    if ((e = cudaEventSynchronize(ev[2])) != cudaSuccess) return cuda_status(c, e, "render");
+    float t1 = 0.f, t2 = 0.f;
+    cudaEventElapsedTime(&t1, ev[0], ev[1]);
+    cudaEventElapsedTime(&t2, ev[1], ev[2]);
+    cam_ms += t1;
+    est_ms += t2;
     render_resolve(a.slots, a.sample_rec, (const float*)c->r_res.ptr, npix, b, q_per_sample,
                    (float4*)c->r_accum.ptr, dropped, st, nullptr, shadow);
     ++passes;
@@ -178,12 +203,13 @@ extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
     render_shadow_compare((const float*)c->q_out.ptr, shadow, npix, std::max(p.spp, 1),
                           max_bits, st);
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(c, e, "render");
-  unsigned long long hd[2] = {0, 0};
+  unsigned long long hd[2] = {0, 0}, hrays = 0;
   int herr = 0;
   unsigned hmax = 0;
   if ((e = cudaMemcpyAsync(out_rgb, c->q_out.ptr, (size_t)npix * 12, cudaMemcpyDeviceToHost,
                            st)) ||
       (e = cudaMemcpyAsync(hd, dropped, 16, cudaMemcpyDeviceToHost, st)) ||
+      (e = cudaMemcpyAsync(&hrays, a.rays, 8, cudaMemcpyDeviceToHost, st)) ||
       (e = cudaMemcpyAsync(&hmax, max_bits, 4, cudaMemcpyDeviceToHost, st)) ||
       (e = cudaMemcpyAsync(&herr, c->dev_err.ptr, 4, cudaMemcpyDeviceToHost, st)) ||
       (e = cudaStreamSynchronize(st)))
@@ -203,6 +229,9 @@ extern "C" int pm_render(pm_ctx* c, const pm_camera* cam,
     float mx = 0.f;
     memcpy(&mx, &hmax, 4);
     stats->accum_rel_err = shadow ? (double)mx : 0.0;
+    stats->rays = (int64_t)hrays;
+    stats->camera_ms = cam_ms;
+    stats->estimate_ms = est_ms;
   }
   return PM_OK;
 }

@@ -127,8 +127,21 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
   unsigned* status = (unsigned*)((char*)c->trace_misc.ptr + 16);
   // capacity guess: 4 stored photons per emitted one; retried when short
   unsigned long long cap = (unsigned long long)(n_emit > 0 ? n_emit : 1) * 4;
-  unsigned long long stored = 0;
+  unsigned long long stored = 0, hrays = 0;
   unsigned hstatus[2] = {0, 0};
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  for (auto& x : ev)
+    if ((e = cudaEventCreate(&x)) != cudaSuccess) {
+      for (auto& y : ev)
+        if (y) cudaEventDestroy(y);
+      return cuda_status(c, e, "trace events");
+    }
+  struct EvGuard {
+    cudaEvent_t* ev;
+    ~EvGuard() {
+      for (int i = 0; i < 3; ++i) cudaEventDestroy(ev[i]);
+    }
+  } guard{ev};
   for (int attempt = 0; attempt < 2; ++attempt) {
     if ((s = c->trace_raw.ensure(cap * 36)) || (s = c->trace_keys.ensure(cap * 8)))
       return set_err(c, s, "trace buffers (%llu photons)", cap);
@@ -145,12 +158,16 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
     a.cap = cap;
     a.status = status;
     a.next = (unsigned long long*)((char*)c->trace_misc.ptr + 32);
+    a.rays = (unsigned long long*)((char*)c->trace_misc.ptr + 48);
     a.dmat = dmat;
+    cudaEventRecord(ev[0], st);
     trace_launch(c->scene_view(), a, st);
+    cudaEventRecord(ev[1], st);
     if ((e = cudaGetLastError()) != cudaSuccess)
       return cuda_status(c, e, "trace launch");
     if ((e = cudaMemcpyAsync(&stored, counter, 8, cudaMemcpyDeviceToHost, st)) ||
         (e = cudaMemcpyAsync(hstatus, status, 8, cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaMemcpyAsync(&hrays, a.rays, 8, cudaMemcpyDeviceToHost, st)) ||
         (e = cudaStreamSynchronize(st)))
       return cuda_status(c, e, "trace");
     if ((s = take_device_error(c, "trace")) != PM_OK) return s;
@@ -176,6 +193,7 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
       return cuda_status(c, e, "photon order");
   }
   if ((s = build_map(c, dm, (const float*)dm.aos.ptr, n, st)) != PM_OK) return s;
+  cudaEventRecord(ev[2], st);
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
     return cuda_status(c, e, "photon map build");
   c->map_emitted[map] = n_emit;
@@ -184,6 +202,11 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
     stats->stored = (int64_t)stored;
     stats->nan_throughput = hstatus[0];
     stats->negative_throughput = hstatus[1];
+    stats->rays = (int64_t)hrays;
+    stats->trace_ms = 0.f;
+    stats->build_ms = 0.f;
+    cudaEventElapsedTime(&stats->trace_ms, ev[0], ev[1]);
+    cudaEventElapsedTime(&stats->build_ms, ev[1], ev[2]);
   }
   return PM_OK;
 }

@@ -39,6 +39,24 @@ int map_levels(int64_t n, int* nlevels, int* lvl_off, int* lvl_cnt) {
   return off;
 }
 
+size_t grid_words(int64_t n, int* lmax, int* off) {
+  // finest level: about one cell per photon or coarser (8^L <= 8 n), at
+  // most kGridMaxLevel; maps too small for kGridMinLevel get no grid
+  int L = 0;
+  while (L < kGridMaxLevel && (int64_t)1 << (3 * (L + 1)) <= 8 * n) ++L;
+  if (n <= 0 || L < kGridMinLevel) {
+    *lmax = 0;
+    return 0;
+  }
+  *lmax = L;
+  size_t w = kGridHeader;
+  for (int l = kGridMinLevel; l <= L; ++l) {
+    off[l - kGridMinLevel] = (int)w;
+    w += ((size_t)1 << (3 * l)) + 1;
+  }
+  return w;
+}
+
 size_t map_build_scratch_bytes(int64_t n) {
   const size_t nn = (size_t)(n > 0 ? n : 1);
   // keys a/b, values a/b, tile histogram, bbox words
@@ -190,10 +208,42 @@ __global__ void node_box_kernel(float4* __restrict__ boxes, int child_off,
   }
 }
 
+// Finest grid level: the first sorted photon of each cell c (the first
+// key >= c << shift), for c in [0, ncells]; cell ncells gets n.
+__global__ void grid_finest_kernel(const uint32_t* __restrict__ keys, int n, int shift,
+                                   uint32_t ncells, uint32_t* __restrict__ tab) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c > ncells) return;
+  if (c == ncells) {
+    tab[c] = (uint32_t)n;
+    return;
+  }
+  const uint32_t want = c << shift;
+  int lo = 0, hi = n;  // lower bound in [lo, hi]
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(keys + mid) < want) lo = mid + 1;
+    else hi = mid;
+  }
+  tab[c] = (uint32_t)lo;
+}
+
+// A coarser level: cell c starts where its first child cell 8c starts.
+__global__ void grid_coarser_kernel(const uint32_t* __restrict__ fine, uint32_t ncells,
+                                    uint32_t* __restrict__ tab) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c <= ncells) tab[c] = fine[(size_t)c << 3];
+}
+
+__global__ void grid_header_kernel(const uint32_t* __restrict__ bb, uint32_t* __restrict__ grid) {
+  if (threadIdx.x < 6) grid[threadIdx.x] = bb[threadIdx.x];
+  else if (threadIdx.x < kGridHeader) grid[threadIdx.x] = 0;
+}
+
 void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
                       float2* wi2, float4* boxes, const int* lvl_off,
                       const int* lvl_cnt, int nlevels, void* scratch,
-                      cudaStream_t st) {
+                      cudaStream_t st, uint32_t* grid, int grid_lmax, const int* grid_off) {
   if (n <= 0) return;
   uint32_t* ka = (uint32_t*)scratch;
   uint32_t* kb = ka + n;
@@ -216,35 +266,28 @@ void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
     node_box_kernel<<<(lvl_cnt[l] * 32 + tb - 1) / tb, tb, 0, st>>>(
         boxes, lvl_off[l - 1], lvl_cnt[l - 1], lvl_off[l], lvl_cnt[l]);
   }
+  if (grid && grid_lmax >= kGridMinLevel) {
+    grid_header_kernel<<<1, 32, 0, st>>>(bb, grid);
+    const uint32_t* keys = in_b ? kb : ka;
+    const int L = grid_lmax;
+    const uint32_t nc = 1u << (3 * L);
+    uint32_t* fine = grid + grid_off[L - kGridMinLevel];
+    grid_finest_kernel<<<(nc + 1 + tb - 1) / tb, tb, 0, st>>>(keys, n, 3 * (10 - L), nc, fine);
+    for (int l = L - 1; l >= kGridMinLevel; --l) {
+      const uint32_t ncl = 1u << (3 * l);
+      uint32_t* tab = grid + grid_off[l - kGridMinLevel];
+      grid_coarser_kernel<<<(ncl + 1 + tb - 1) / tb, tb, 0, st>>>(fine, ncl, tab);
+      fine = tab;
+    }
+  }
 }
 
 // -------------------------------------------------------------- kNN query
 //
-// One warp answers the queries of a work item (16 consecutive queries, 8 at
-// the end of a launch; the batched kernel takes `chunk`), 32 at a time in a
-// window whose query records sit in the lanes' registers (lane i holds
-// query i of the window).
-//
-// Neighbourhood pools (k <= kPoolMaxK). Queries close to each other share
-// most of their neighbours, so one tree walk serves a group of them. A
-// group is every pending query of the window within kPoolGroup x r of the
-// first pending one (r: the last exact k-th distance the warp found). The
-// walk collects every photon within R = kPoolFactor x r + rc of the
-// group's centre (rc: the largest distance of a member from it) into a pool
-// in shared memory: position and sorted position, at most P photons. A
-// member at distance rq from the centre needs no photon outside the pool
-// when its k-th distance is at most R - rq (triangle inequality, with
-// rounding margins): it computes its distance to every pool photon (one
-// register per 32 photons), finds the exact k-th (dist2, index) pair with
-// a 256-bin histogram of the distances over [0, (R - rq)^2] and a rank of
-// the critical bin, and keeps the pool photons below it. A member that
-// fails the test (fewer than k pool photons within R - rq, or a critical
-// bin of more than 32 photons), and every member of a group whose pool
-// overflowed, is answered by the per-query search afterwards.
-//
-// Per-query search:
+// One warp answers one query at a time, walking a chunk of consecutive
+// queries. Per query:
 //   1. bound: an upper bound tau of the k-th distance. From the previous
-//      query answered this way by the triangle inequality when it is close
+//      query of the chunk by the triangle inequality when it is close
 //      ((r_prev + delta)^2, inflated for rounding; first tried at the
 //      smaller (1.06 r_prev)^2, kept when it holds k photons), else from
 //      the photons Morton-adjacent to the group nearest the query.
@@ -252,13 +295,9 @@ void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
 //      8-photon groups of a node are scanned packed, 4 groups per round,
 //      every photon with dist2 <= tau appended to the warp's buffer. A
 //      nearly full buffer is cut to the k best, lowering tau.
-//   3. select: exact k-th (dist2, index) pair (histogram, else radix).
-// Both ways give the kept photons in the order of the tree's depth-first
-// walk: a fixed total order of the photons that no bound changes (a pool
-// and a search buffer list the photons they hold in that order, and the
-// cuts keep it). The radiance sum over them (Lambert, integrator.h:141-150)
-// therefore does not depend on how a query was answered, nor on the order
-// queries come in.
+//   3. select: radix select of the exact k-th (dist2, index) pair.
+//   4. output: the radiance sum (Lambert, integrator.h:141-150) or the
+//      index list in the reference's order.
 
 constexpr int kStack = 32 * kMaxLevels;
 
@@ -272,51 +311,60 @@ constexpr float kWarmGuess = 1.06f;
 // Work items of the persistent launch: kChunk consecutive queries per
 // work-counter bump, then kTail queries per bump for the last
 // kTailItems x (resident warps) x kTail queries, so that the warps run out
-// of work at nearly the same time.
+// of work at nearly the same time (measured on 1M primary-hit queries at
+// k = 100: 3.68 ms against 3.96 ms with items of 32 throughout; larger
+// items keep more warm starts but leave a longer tail).
 constexpr int kChunk = 16;
 constexpr int kTail = 8;
 constexpr int kTailItems = 2;
 static_assert(kChunk % 8 == 0 && kTail % 8 == 0, "items start at multiples of 8");
-static_assert(kChunk <= 32 && kTail <= kChunk, "an item fits one window");
 
-// Pools: k up to kPoolMaxK (the kept list of a pool query, keys and sorted
-// positions, lives in the 256 words of the histogram); group radius and
-// pool radius in units of the last k-th distance.
-constexpr int kPoolMaxK = 128;
-constexpr float kPoolGroup = 0.6f;
-constexpr float kPoolFactor = 1.15f;
-// Photons held by a pool in the kernels that pool (16 B each, in the space
-// of the search buffer), and that search buffer's size.
-constexpr int kPoolSize = 512;
-constexpr int kPoolBuf = 1024;
-static_assert(kPoolSize * 16 <= kPoolBuf * 8, "the pool fits the search buffer");
-
-// Entries of the search buffer kept free for the next append round and the
-// cut: a buffer holding more than C - kCutSlack candidates is cut.
-constexpr int kCutSlack = 56;
+// The last kStageWords entries of WarpBuf::id hold the radiance of up to 8
+// consecutive queries (an aligned group of 8) until the warp stores them
+// together: 96 bytes in six 16-byte stores instead of 24 scattered words,
+// which matters when the output is mapped host memory.
+constexpr int kStageWords = 24;
 
 template <int C>
 struct WarpBuf {
-  uint32_t key[C];  // float bits of dist2 (non-negative: order == uint order);
-                    // with id[], also the pool (float4 {position, sorted position})
+  uint32_t key[C];  // float bits of dist2 (non-negative: order == uint order)
   uint32_t id[C];   // sorted position of the photon
-  uint32_t hist[256];  // selection histogram; the kept list of a pool query
+  uint32_t hist[256];
   uint32_t stack[kStack];
-  uint32_t list[64];   // passing groups waiting to be scanned, in walk order
-  uint32_t sel[32];    // entries of the critical bin of a selection
-  uint32_t stat[8];    // per-warp counters, same order as pm_knn_stats
-  float stage[3 * kChunk];  // radiance of the current work item (host path)
+  uint32_t list[64];  // passing groups waiting to be scanned, in walk order
+  uint32_t sel[32];   // entries of the critical bin of a selection
+  uint32_t stat[8];   // per-warp counters, same order as pm_knn_stats
+  float4 rec[2][3];   // radiance records of this query and the next (cp.async)
 };
+
+// 16-byte asynchronous copy global -> shared (the source may be mapped host
+// memory), and the waits on it (per thread).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;\n" ::: "memory");
+}
 
 struct Levels {
   int2 oc[kMaxLevels];  // {offset of the level's boxes, boxes in the level}
+  // the cell grid: finest level (0: not used), word offsets of the levels'
+  // tables, the box the Morton codes were made in, its smallest positive
+  // extent
+  int glmax;
+  int goff[kGridLevels];
+  float glo[3], gext[3];
+  float gmin_ext;
 };
 
 enum {
   kStatQueries = 0, kStatCold, kStatCand, kStatLeaves, kStatNodes, kStatSelects, kStatWalks,
-  kStatPoolQueries, kNumStats
+  kStatGrid, kNumStats
 };
-static_assert(kNumStats <= 8, "stat[] holds the counters");
 
 // Counters are compiled in only for the kernels launched with statistics.
 template <bool S, int C>
@@ -418,12 +466,11 @@ __device__ uint32_t warp_select(uint32_t* hist, int cnt, uint32_t kk, Get get,
 }
 
 // Finds the bin holding the kk-th smallest entry of a 256-bin histogram
-// already filled: returns the bin; *kk_in = rank inside it (1-based),
-// *n_bin = entries in it, *total = entries in all bins. When *total < kk
-// the other outputs are 0.
+// already filled (sum >= kk): returns the bin; *kk_in = rank inside it
+// (1-based), *n_bin = entries in it.
 __device__ __forceinline__ uint32_t hist_find(const uint32_t* hist, uint32_t kk,
                                               int lane, uint32_t* kk_in,
-                                              uint32_t* n_bin, uint32_t* total) {
+                                              uint32_t* n_bin) {
   uint32_t h[8];
   uint32_t sum = 0;
 #pragma unroll
@@ -436,12 +483,6 @@ __device__ __forceinline__ uint32_t hist_find(const uint32_t* hist, uint32_t kk,
   for (int o = 1; o < 32; o <<= 1) {
     const uint32_t t = __shfl_up_sync(kFull, incl, o);
     if (lane >= o) incl += t;
-  }
-  *total = __shfl_sync(kFull, incl, 31);
-  if (*total < kk) {
-    *kk_in = 0;
-    *n_bin = 0;
-    return 0;
   }
   const uint32_t excl = incl - sum;
   const unsigned owner = __ballot_sync(kFull, excl < kk && kk <= incl);
@@ -469,29 +510,6 @@ __device__ __forceinline__ uint32_t hist_find(const uint32_t* hist, uint32_t kk,
   return __shfl_sync(kFull, bin, ol);
 }
 
-// The k-th (key, original index) pair among the nb <= 32 entries of a
-// critical bin held by lanes 0..nb-1 (kj, oj; other lanes ~0): rank kk
-// (1-based) among them. Returns kth_key; *kth_oid = the pair's index, or
-// 0xffffffff when no other entry of the bin has that key (every entry with
-// the key is then kept).
-__device__ __forceinline__ uint32_t rank_critical(uint32_t kj, uint32_t oj, int nb, uint32_t kk,
-                                                  int lane, uint32_t* kth_oid) {
-  int rank = 0;
-  for (int t = 0; t < nb; ++t) {
-    const uint32_t kt = __shfl_sync(kFull, kj, t);
-    const uint32_t ot = __shfl_sync(kFull, oj, t);
-    rank += (kt < kj) || (kt == kj && ot < oj);
-  }
-  const unsigned who = __ballot_sync(kFull, lane < nb && rank == (int)kk - 1);
-  const int wl = __ffs(who) - 1;
-  const uint32_t kth_key = __shfl_sync(kFull, kj, wl);
-  uint32_t oid = __shfl_sync(kFull, oj, wl);
-  const unsigned same = __ballot_sync(kFull, lane < nb && kj == kth_key);
-  if (__popc(same) == 1) oid = 0xffffffffu;
-  *kth_oid = oid;
-  return kth_key;
-}
-
 // Fast exact selection for a buffer whose dist2 all lie in [0, tau]:
 // one histogram of dist2 over 256 equal bins of [0, tau] (bin = floor(d2 *
 // 256/tau) is monotone in d2, so every entry of a lower bin is smaller),
@@ -516,9 +534,9 @@ __device__ __forceinline__ bool select_kth_hist(const float4* pos4,
     atomicAdd(&s.hist[b], 1u);
   }
   __syncwarp();
-  uint32_t kk, nb, total;
-  const int bin = (int)hist_find(s.hist, (uint32_t)k, lane, &kk, &nb, &total);
-  if (total < (uint32_t)k || nb > 32) return false;
+  uint32_t kk, nb;
+  const int bin = (int)hist_find(s.hist, (uint32_t)k, lane, &kk, &nb);
+  if (nb > 32) return false;
   int pos = 0;
   for (int base = 0; base < cnt; base += 32) {
     const int i = base + lane;
@@ -537,7 +555,19 @@ __device__ __forceinline__ bool select_kth_hist(const float4* pos4,
     kj = s.key[i];
     oj = orig_index(pos4, s.id[i]);
   }
-  kth_key = rank_critical(kj, oj, (int)nb, kk, lane, &kth_oid);
+  int rank = 0;
+  for (int t = 0; t < (int)nb; ++t) {
+    const uint32_t kt = __shfl_sync(kFull, kj, t);
+    const uint32_t ot = __shfl_sync(kFull, oj, t);
+    rank += (kt < kj) || (kt == kj && ot < oj);
+  }
+  const unsigned who = __ballot_sync(kFull, lane < (int)nb && rank == (int)kk - 1);
+  const int wl = __ffs(who) - 1;
+  kth_key = __shfl_sync(kFull, kj, wl);
+  kth_oid = __shfl_sync(kFull, oj, wl);
+  // a key held by one entry only: keep every entry with that key
+  const unsigned same = __ballot_sync(kFull, lane < (int)nb && kj == kth_key);
+  if (__popc(same) == 1) kth_oid = 0xffffffffu;
   __syncwarp();
   return true;
 }
@@ -607,11 +637,11 @@ __device__ __forceinline__ int compact_kept(const float4* pos4, WarpBuf<C>& s,
   return dst;
 }
 
-// State of a search walk.
+// Per-query state of the search.
 struct Query {
   float x, y, z;
   float tau;  // every photon with dist2 <= tau is collected
-  int cnt;    // entries in the warp buffer (or the pool)
+  int cnt;    // entries in the warp buffer
   int k;
 };
 
@@ -627,34 +657,22 @@ __device__ __forceinline__ uint2 tighten(const float4* pos4, WarpBuf<C>* sp,
   return make_uint2((uint32_t)n2, kth_key);
 }
 
-// Appends photon i (position p) when valid and dist2 <= tau.
-// P == 0: to the search buffer ({dist2, sorted position}); when the buffer
-//         is nearly full, keeps the k best and lowers tau to the k-th.
-// P > 0:  to the pool ({position, sorted position} as float4); entries past
-//         P are counted but not written (the caller sees q.cnt > P).
-template <int C, int P, bool S>
+// Appends photon i (position p) when valid and dist2 <= tau. When the
+// buffer is nearly full, keeps the k best and lowers tau to the k-th.
+template <int C, bool S>
 __device__ __forceinline__ void offer(const MapDev& m, Query& q, WarpBuf<C>& s,
                                       int lane, const float4& p, int i,
                                       bool valid) {
   const float d2 = dist2_ref(q.x, q.y, q.z, p.x, p.y, p.z);
   const bool pass = valid && d2 <= q.tau;
   const unsigned bal = __ballot_sync(kFull, pass);
-  if (P > 0) {
-    if (pass) {
-      const int o = q.cnt + __popc(bal & lanemask_lt());
-      if (o < P)
-        reinterpret_cast<float4*>(s.key)[o] = make_float4(p.x, p.y, p.z, __uint_as_float((uint32_t)i));
-    }
-    q.cnt += __popc(bal);
-    return;
-  }
   if (pass) {
     const int o = q.cnt + __popc(bal & lanemask_lt());
     s.key[o] = __float_as_uint(d2);
     s.id[o] = (uint32_t)i;
   }
   q.cnt += __popc(bal);
-  if (q.cnt > C - kCutSlack) {
+  if (q.cnt > C - 32 - kStageWords) {
     __syncwarp();
     const uint2 r = tighten<C, S>(m.pos4, &s, q.cnt, q.k, q.tau, lane);
     q.cnt = (int)r.x;
@@ -665,7 +683,7 @@ __device__ __forceinline__ void offer(const MapDev& m, Query& q, WarpBuf<C>& s,
 // Scans the photons of the ng groups listed in s.list: lane l handles
 // photon (l & 7) of group 4r + (l >> 3) in round r; two rounds are loaded
 // before either is used.
-template <int C, int P, bool S>
+template <int C, bool S>
 __device__ __forceinline__ void scan_groups(const MapDev& m, Query& q,
                                             WarpBuf<C>& s, int lane, int ng) {
   const int sub = lane >> 3, j = lane & 7;
@@ -681,14 +699,14 @@ __device__ __forceinline__ void scan_groups(const MapDev& m, Query& q,
     float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
     if (va) pa = __ldg(m.pos4 + ia);
     if (vb) pb = __ldg(m.pos4 + ib);
-    offer<C, P, S>(m, q, s, lane, pa, ia, va);
-    if (r + 4 < ng) offer<C, P, S>(m, q, s, lane, pb, ib, vb);
+    offer<C, S>(m, q, s, lane, pa, ia, va);
+    if (r + 4 < ng) offer<C, S>(m, q, s, lane, pb, ib, vb);
   }
   __syncwarp();
 }
 
 // Scans the contiguous photon range [lo, hi), 32 photons per round.
-template <int C, int P, bool S>
+template <int C, bool S>
 __device__ __forceinline__ void scan_range(const MapDev& m, Query& q,
                                            WarpBuf<C>& s, int lane, int lo,
                                            int hi) {
@@ -698,25 +716,25 @@ __device__ __forceinline__ void scan_range(const MapDev& m, Query& q,
     float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
     if (va) pa = __ldg(m.pos4 + ia);
     if (vb) pb = __ldg(m.pos4 + ib);
-    offer<C, P, S>(m, q, s, lane, pa, ia, va);
-    if (b + 32 < hi) offer<C, P, S>(m, q, s, lane, pb, ib, vb);
+    offer<C, S>(m, q, s, lane, pa, ia, va);
+    if (b + 32 < hi) offer<C, S>(m, q, s, lane, pb, ib, vb);
   }
 }
 
 // Depth-first walk of the box tree collecting all photons with
-// dist2 <= q.tau into the warp buffer (P == 0) or the pool (P > 0; the walk
-// stops once more than P photons were found). Passing 8-photon groups join
-// a waiting list, scanned in full rounds of 8 as they accumulate and in
-// full once the walk ends. Both go through one scan site: the scan inlines
-// the candidate appends and the rare buffer cut, and a second copy of it
-// made the kernel 1.9 % slower (same scan order, same results).
-template <int C, int P, bool S>
+// dist2 <= q.tau into the warp buffer. Passing 8-photon groups join a
+// waiting list, scanned in full rounds of 8 as they accumulate and in full
+// once the walk ends. Both go through one scan site: the scan inlines the
+// candidate appends and the rare buffer cut, and a second copy of it made
+// the kernel 1.9 % slower (3.387 against 3.324 ms on 1M primary-hit queries
+// at k = 100; same scan order, same results).
+template <int C, bool S>
 __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
                                         Query& q, WarpBuf<C>& s, int lane) {
   q.cnt = 0;
   stat_add<S>(s, lane, kStatWalks, 1);
   if (m.nlevels == 1) {  // a single 8-photon group
-    scan_range<C, P, S>(m, q, s, lane, 0, m.n);
+    scan_range<C, S>(m, q, s, lane, 0, m.n);
     return;
   }
   if (lane == 0) s.stack[0] = ((uint32_t)(m.nlevels - 1) << 28);
@@ -752,7 +770,7 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
     // full rounds of 8 groups after a bottom-level node, the rest at the end
     const int take = done ? pending : (cl == 0 ? (pending & ~7) : 0);
     if (take > 0) {
-      scan_groups<C, P, S>(m, q, s, lane, take);
+      scan_groups<C, S>(m, q, s, lane, take);
       const int rest = pending - take;
       uint32_t keep = 0;
       if (lane < rest) keep = s.list[take + lane];
@@ -760,10 +778,183 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
       if (lane < rest) s.list[lane] = keep;
       __syncwarp();
       pending = rest;
-      if (P > 0 && q.cnt > P) break;  // the pool overflowed
     }
     if (done) break;
   }
+}
+
+// Photons per bottom node of the box tree (32 groups of 8).
+constexpr int kNodeSpan = 32 * kGroup;
+
+__device__ __forceinline__ unsigned lanemask_le() {
+  unsigned m;
+  asm volatile("mov.u32 %0, %%lanemask_le;" : "=r"(m));
+  return m;
+}
+
+// Candidates from the cell grid: every photon with dist2 <= q.tau into the
+// warp buffer, in the order the tree walk meets them (bottom nodes of
+// kNodeSpan sorted photons in descending order, photons ascending within
+// one), so the kept photons, their order and their sum do not depend on
+// which of the two ran. Returns false, having appended nothing, when the
+// grid does not suit the radius r and the tree is walked instead:
+//   * the level is the finest whose cells are at least 2r/3 along every
+//     axis (so the query's box, 2r wide, meets at most 4 cells per axis,
+//     64 in all); it must not be coarser than kGridMinLevel;
+//   * the map's finest level must not be coarser than that by 2 levels or
+//     more (cells many times the sphere: the tree tests fewer photons);
+//   * the candidate cells must give at most 32 pieces (below).
+// The candidate cells are the build's own cells of q -+ r per axis (the
+// same cell function, with a margin for the rounding of q -+ r); a cell
+// whose box (widened by 1e-3 of a cell) is farther than sqrt(tau) is
+// skipped. A cell is one range of sorted photons, cut into pieces at
+// bottom-node boundaries; the pieces are ranked in the walk's order and
+// scanned as one stream, 32 photons per round.
+template <int C, bool S>
+__device__ __forceinline__ bool collect_grid(const MapDev& m, const Levels& L, Query& q,
+                                             WarpBuf<C>& s, int lane) {
+  const float r = sqrtf(q.tau);
+  if (!(r > 0.f) || !(r < __int_as_float(0x7f800000)) || !(fabsf(q.x) < 1e30f) ||
+      !(fabsf(q.y) < 1e30f) || !(fabsf(q.z) < 1e30f))
+    return false;
+  const float rr = r * 1.0001f;
+  const int lv = ilogbf(__fdividef(1.5f * L.gmin_ext, rr));
+  if (lv < kGridMinLevel || lv >= L.glmax + 2) return false;
+  const int lvl = min(lv, L.glmax);
+  const int sh = 10 - lvl;
+  int c0[3], nc[3];
+  const float qv[3] = {q.x, q.y, q.z};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float mg = rr + fabsf(qv[a]) * 1e-6f;
+    c0[a] = (int)(cell10(qv[a] - mg, L.glo[a], L.gext[a]) >> sh);
+    nc[a] = (int)(cell10(qv[a] + mg, L.glo[a], L.gext[a]) >> sh) - c0[a] + 1;
+  }
+  if (nc[0] > 4 || nc[1] > 4 || nc[2] > 4) return false;
+  const float scale = __int_as_float((127 - lvl) << 23);  // 2^-lvl
+  const uint32_t* tab = m.grid + L.goff[lvl - kGridMinLevel];
+  // the candidate cells (slot t of 4 x 4 x 4 is (t & 3, t >> 2 & 3, t >> 4)),
+  // cut into pieces at bottom-node boundaries: s.stack[0..32) starts,
+  // s.stack[32..64) ends
+  int npc = 0;
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    const int t = lane + 32 * h;
+    const int dx = t & 3, dy = (t >> 2) & 3, dz = t >> 4;
+    bool use = dx < nc[0] && dy < nc[1] && dz < nc[2];
+    uint32_t b = 0, e = 0;
+    if (use) {
+      const int cx = c0[0] + dx, cy = c0[1] + dy, cz = c0[2] + dz;
+      const float sx = L.gext[0] * scale, sy = L.gext[1] * scale, sz = L.gext[2] * scale;
+      const float4 blo = make_float4(L.glo[0] + (float)cx * sx - sx * 1e-3f,
+                                     L.glo[1] + (float)cy * sy - sy * 1e-3f,
+                                     L.glo[2] + (float)cz * sz - sz * 1e-3f, 0.f);
+      const float4 bhi = make_float4(L.glo[0] + (float)(cx + 1) * sx + sx * 1e-3f,
+                                     L.glo[1] + (float)(cy + 1) * sy + sy * 1e-3f,
+                                     L.glo[2] + (float)(cz + 1) * sz + sz * 1e-3f, 0.f);
+      use = box_dist2(q.x, q.y, q.z, blo, bhi) <= q.tau;
+      if (use) {
+        const uint32_t code = (spread10((uint32_t)cx) << 2) | (spread10((uint32_t)cy) << 1) |
+                              spread10((uint32_t)cz);
+        b = __ldg(tab + code);
+        e = __ldg(tab + code + 1);
+        use = e > b;
+      }
+    }
+    const int cnt = use ? (int)(((e - 1) / kNodeSpan) - (b / kNodeSpan)) + 1 : 0;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(kFull, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const int tot = __shfl_sync(kFull, incl, 31);
+    if (npc + tot <= 32) {
+      int o = npc + incl - cnt;
+      for (uint32_t x = b; x < e; ++o) {
+        const uint32_t xe = min(e, (x / kNodeSpan + 1) * kNodeSpan);
+        s.stack[o] = x;
+        s.stack[32 + o] = xe;
+        x = xe;
+      }
+    }
+    npc += tot;
+  }
+  if (npc > 32) return false;
+  __syncwarp();
+  // rank the pieces in the walk's order, then piece j in lane j
+  uint32_t pb = 0, pe = 0, key = 0xffffffffu;
+  if (lane < npc) {
+    pb = s.stack[lane];
+    pe = s.stack[32 + lane];
+    key = ((0x7fffffu - pb / kNodeSpan) << 8) | (pb % kNodeSpan);
+  }
+  int rank = 0;
+  for (int t = 0; t < npc; ++t) rank += __shfl_sync(kFull, key, t) < key;
+  if (lane < npc) {
+    s.stack[64 + rank] = pb;
+    s.stack[96 + rank] = pe;
+  }
+  __syncwarp();
+  uint32_t sb = 0, len = 0;
+  if (lane < npc) {
+    sb = s.stack[64 + lane];
+    len = s.stack[96 + lane] - sb;
+  }
+  uint32_t incl = len;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(kFull, incl, o);
+    if (lane >= o) incl += y;
+  }
+  const uint32_t total = __shfl_sync(kFull, incl, 31);
+  const uint32_t off = incl - len;  // stream offset of piece `lane`
+  q.cnt = 0;
+  stat_add<S>(s, lane, kStatWalks, 1);
+  stat_add<S>(s, lane, kStatGrid, 1);
+  stat_add<S>(s, lane, kStatLeaves, (uint32_t)npc);
+  // the stream, two rounds of 32 loaded before either is offered; the
+  // piece of stream index t is the last piece starting at or before t
+  int before = 0;
+  for (uint32_t r0 = 0; r0 < total; r0 += 64) {
+    int ia = 0, ib = 0;
+    bool va, vb;
+    {
+      const uint32_t bit = lane < npc && off >= r0 && off < r0 + 32 ? 1u << (off - r0) : 0u;
+      const uint32_t starts = __reduce_or_sync(kFull, bit);
+      const int j = before + __popc(starts & lanemask_le()) - 1;
+      before += __popc(starts);
+      const uint32_t t = r0 + lane;
+      va = t < total;
+      ia = (int)(__shfl_sync(kFull, sb, j & 31) + (t - __shfl_sync(kFull, off, j & 31)));
+    }
+    {
+      const uint32_t r1 = r0 + 32;
+      const uint32_t bit = lane < npc && off >= r1 && off < r1 + 32 ? 1u << (off - r1) : 0u;
+      const uint32_t starts = __reduce_or_sync(kFull, bit);
+      const int j = before + __popc(starts & lanemask_le()) - 1;
+      before += __popc(starts);
+      const uint32_t t = r1 + lane;
+      vb = t < total;
+      ib = (int)(__shfl_sync(kFull, sb, j & 31) + (t - __shfl_sync(kFull, off, j & 31)));
+    }
+    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pbv = pa;
+    if (va) pa = __ldg(m.pos4 + ia);
+    if (vb) pbv = __ldg(m.pos4 + ib);
+    offer<C, S>(m, q, s, lane, pa, ia, va);
+    if (r0 + 32 < total) offer<C, S>(m, q, s, lane, pbv, ib, vb);
+  }
+  __syncwarp();
+  return true;
+}
+
+// Candidates of query q: from the cell grid when it suits, else by the
+// tree walk.
+template <int C, bool S>
+__device__ __forceinline__ void gather(const MapDev& m, const Levels& L, Query& q,
+                                       WarpBuf<C>& s, int lane) {
+  if (L.glmax > 0 && collect_grid<C, S>(m, L, q, s, lane)) return;
+  collect<C, S>(m, L, q, s, lane);
 }
 
 __device__ __forceinline__ unsigned long long warp_min_u64(
@@ -816,7 +1007,7 @@ __device__ __forceinline__ float cold_tau(const float4* pos4, const float4* boxe
   const int want = min(ngroups, max(32, (k + kGroup - 1) / kGroup + 8));
   const int first =
       max(0, min(want == 32 ? (node & ~31) : node - want / 2, ngroups - want));
-  scan_range<C, 0, S>(m, q, s, lane, first * kGroup, min(n, (first + want) * kGroup));
+  scan_range<C, S>(m, q, s, lane, first * kGroup, min(n, (first + want) * kGroup));
   __syncwarp();
   if (q.cnt < k) return __int_as_float(0x7f800000);
   uint32_t mx = 0;
@@ -827,479 +1018,298 @@ __device__ __forceinline__ float cold_tau(const float4* pos4, const float4* boxe
   return __uint_as_float(kth_key);
 }
 
-// Warm state of the per-query search: the previous query answered this way
-// and its exact k-th distance.
-struct Warm {
-  bool have;
-  float x, y, z, kth;
-};
-
-// Per-query search of query (qx, qy, qz): the kept photons (the k nearest,
-// or all photons when fewer), compacted in s.key / s.id in walk order.
-// Returns their number; *maxd2 = the largest kept dist2 (0 when none).
+// Answers queries [qb, qe) of a work item on map m, one at a time (one warp).
 // r_hint: the last exact k-th distance this warp found (in/out).
-template <int C, bool S>
-__device__ __forceinline__ int search_one(const MapDev& m, const Levels& L, WarpBuf<C>& s,
-                                          int lane, float qx, float qy, float qz, int k,
-                                          Warm& w, float& r_hint, float* maxd2) {
+// HIO (the single-map kernel, whose queries and output may be mapped host
+// memory): radiance records are prefetched one query ahead with cp.async,
+// and without `order` the radiance goes out in aligned groups of 8 queries.
+// Without HIO (the batched kernel, device-resident slots) records are read
+// with plain loads: measured on the 64-scene batch, the prefetch and the
+// staging code together cost it 13 % through register allocation.
+template <int C, int MODE, bool S, bool HIO>
+__device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, WarpBuf<C>& s,
+                                          int lane, const void* __restrict__ queries,
+                                          int64_t qb, int64_t qe, int k, float n_emitted,
+                                          const KnnOut& out, const uint32_t* __restrict__ order,
+                                          int stride4, float& r_hint) {
   const float kInf = __int_as_float(0x7f800000);
-  Query q;
-  q.x = qx; q.y = qy; q.z = qz;
-  q.k = k;
-  q.cnt = 0;
-  q.tau = kInf;
-  const bool bad = m.n == 0 || isnan(qx) || isnan(qy) || isnan(qz);
-  if (!bad) {
-    bool warm = false, warm_guess = false;
-    float tau_sure = 0.f;
-    if (w.have) {
-      const float d2 = dist2_ref(qx, qy, qz, w.x, w.y, w.z);
-      if (d2 <= w.kth) {
-        const float rp = sqrtf(w.kth);
-        const float r = rp + sqrtf(d2);
-        const float rr = r * 1.00001f;
-        tau_sure = fmaxf(rr * rr * 1.00001f, 1e-37f);
-        q.tau = tau_sure;
-        warm = true;
-        // the k-th distance changes little between neighbours: collect
-        // within a radius a little above the previous one first; fewer
-        // than k photons inside it falls back to the sure bound
-        const float rg = kWarmGuess * rp;
-        if (rg * rg < tau_sure) {
-          q.tau = rg * rg;
-          warm_guess = true;
+  bool have_prev = false;
+  float pqx = 0.f, pqy = 0.f, pqz = 0.f, pkth = 0.f;
+  // HIO: the three float4 of a radiance record are staged in s.rec by lanes
+  // 0-2 one query ahead, so the load (from device or mapped host memory)
+  // overlaps the previous query's search.
+  auto fetch = [&](int64_t qn, int b) {
+    if (lane < 3) {
+      const int64_t rn = order ? (int64_t)__ldg(order + qn) : qn;
+      cp_async16(&s.rec[b][lane], reinterpret_cast<const float4*>(queries) + stride4 * rn + lane);
+    }
+    cp_async_commit();
+  };
+  int buf = 0;
+  if (MODE != kModeKnn && HIO) fetch(qb, 0);
+  for (int64_t qi = qb; qi < qe; ++qi, buf ^= 1) {
+    Query q;
+    q.k = k;
+    q.cnt = 0;
+    q.tau = kInf;
+    const int64_t rec = (MODE != kModeKnn && order) ? (int64_t)__ldg(order + qi) : qi;
+    if (MODE != kModeKnn && !HIO) {
+      const float4 r0 = __ldg(reinterpret_cast<const float4*>(queries) + stride4 * rec);
+      q.x = r0.x; q.y = r0.y; q.z = r0.z;
+    } else if (MODE != kModeKnn) {
+      cp_async_wait_all();
+      __syncwarp();  // this record is visible; every lane is done with the other buffer
+      if (qi + 1 < qe) fetch(qi + 1, buf ^ 1);
+      // r0 = {pos, rho.r}; wo, ns and the other albedo channels are read
+      // after the search
+      const float4 r0 = s.rec[buf][0];
+      q.x = r0.x; q.y = r0.y; q.z = r0.z;
+    } else {
+      const float* q3 = reinterpret_cast<const float*>(queries) + 3 * qi;
+      q.x = __ldg(q3);
+      q.y = __ldg(q3 + 1);
+      q.z = __ldg(q3 + 2);
+    }
+
+    const bool bad = m.n == 0 || isnan(q.x) || isnan(q.y) || isnan(q.z);
+    if (!bad) {
+      bool warm = false, warm_guess = false;
+      float tau_sure = 0.f;
+      if (have_prev) {
+        const float d2 = dist2_ref(q.x, q.y, q.z, pqx, pqy, pqz);
+        if (d2 <= pkth) {
+          const float rp = sqrtf(pkth);
+          const float r = rp + sqrtf(d2);
+          const float rr = r * 1.00001f;
+          tau_sure = fmaxf(rr * rr * 1.00001f, 1e-37f);
+          q.tau = tau_sure;
+          warm = true;
+          // the k-th distance changes little between neighbours: collect
+          // within a radius a little above the previous one first; fewer
+          // than k photons inside it falls back to the sure bound
+          const float rg = kWarmGuess * rp;
+          if (rg * rg < tau_sure) {
+            q.tau = rg * rg;
+            warm_guess = true;
+          }
+        }
+      }
+      // Guess and verify when no bound is known: collect with a radius a
+      // little above the last k-th distance this warp found; k photons or
+      // more inside it make the result exact, otherwise the radius
+      // doubles (twice), then the patch bound of cold_tau is used.
+      bool guess = false, need_cold = false;
+      float rg = 0.f;
+      if (!warm) {
+        stat_add<S>(s, lane, kStatCold, 1);
+        if (r_hint > 0.f) {
+          guess = true;
+          rg = 1.3f * r_hint;
+          q.tau = fmaxf(rg * rg, 1e-37f);
+        } else {
+          need_cold = true;
+        }
+      }
+      for (int attempt = 0;; ++attempt) {
+        if (need_cold) {
+          q.tau = cold_tau<C, S>(m.pos4, m.boxes, m.n, m.nlevels, &L, q.x, q.y,
+                                 q.z, k, &s, lane);
+          need_cold = false;
+          guess = false;
+        }
+        gather<C, S>(m, L, q, s, lane);
+        if (warm_guess) {
+          if (q.cnt >= k) break;
+          warm_guess = false;
+          q.tau = tau_sure;
+          continue;
+        }
+        if (!guess || q.cnt >= k) break;
+        if (attempt < 2) {
+          rg *= 2.0f;
+          q.tau = fmaxf(rg * rg, 1e-37f);
+        } else {
+          need_cold = true;
         }
       }
     }
-    // Guess and verify when no bound is known: collect with a radius a
-    // little above the last k-th distance this warp found; k photons or
-    // more inside it make the result exact, otherwise the radius doubles
-    // (twice), then the patch bound of cold_tau is used.
-    bool guess = false, need_cold = false;
-    float rg = 0.f;
-    if (!warm) {
-      stat_add<S>(s, lane, kStatCold, 1);
-      if (r_hint > 0.f) {
-        guess = true;
-        rg = 1.3f * r_hint;
-        q.tau = fmaxf(rg * rg, 1e-37f);
-      } else {
-        need_cold = true;
-      }
-    }
-    for (int attempt = 0;; ++attempt) {
-      if (need_cold) {
-        q.tau = cold_tau<C, S>(m.pos4, m.boxes, m.n, m.nlevels, &L, qx, qy, qz, k, &s, lane);
-        need_cold = false;
-        guess = false;
-      }
-      collect<C, 0, S>(m, L, q, s, lane);
-      if (warm_guess) {
-        if (q.cnt >= k) break;
-        warm_guess = false;
-        q.tau = tau_sure;
-        continue;
-      }
-      if (!guess || q.cnt >= k) break;
-      if (attempt < 2) {
-        rg *= 2.0f;
-        q.tau = fmaxf(rg * rg, 1e-37f);
-      } else {
-        need_cold = true;
-      }
-    }
-  }
-  __syncwarp();
-  stat_add<S>(s, lane, kStatQueries, 1);
-  stat_add<S>(s, lane, kStatCand, (uint32_t)q.cnt);
-  const int cnt = q.cnt;
-  const bool all = cnt <= k;
-  uint32_t kth_key = 0, kth_oid = 0xffffffffu;
-  if (all) {
-    uint32_t mx = 0;
-    for (int i = lane; i < cnt; i += 32) mx = max(mx, s.key[i]);
-    kth_key = __reduce_max_sync(kFull, mx);
-  } else {
-    select_kth<C, S>(m.pos4, s, cnt, k, q.tau, lane, kth_key, kth_oid);
-  }
-  const int kept = all ? cnt : k;
-  *maxd2 = kept > 0 ? __uint_as_float(kth_key) : 0.f;
-  const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
-  if (!bad && kept >= k) {
-    w.have = true;
-    w.x = qx; w.y = qy; w.z = qz;
-    w.kth = *maxd2;
-    r_hint = sqrtf(*maxd2);
-  } else {
-    w.have = false;
-  }
-  return nk;
-}
-
-// A query answered from a pool of np photons collected within radius
-// sqrt(tau) of (cx, cy, cz); rp = sqrt(tau) shrunk for rounding. On success
-// the kept photons (exactly k) are in kkey / kid (the histogram's words) in
-// pool order, and *maxd2 is the k-th distance; false when the pool cannot
-// prove the result (the query is then searched on its own).
-template <int C, int P, bool S>
-__device__ __forceinline__ bool pool_query(const MapDev& m, WarpBuf<C>& s, int lane, int np,
-                                           float qx, float qy, float qz, float cx, float cy,
-                                           float cz, float rp, int k, float* maxd2) {
-  const float4* pool = reinterpret_cast<const float4*>(s.key);
-  // every photon within a of the query lies in the pool: |p - c| <=
-  // |p - q| + |q - c| <= a + rq <= rp, with margins of 1e-5 relative for
-  // the rounding of the distances (a few units of 2^-24 each)
-  const float rq = sqrtf(dist2_ref(qx, qy, qz, cx, cy, cz)) * 1.00001f;
-  const float a = rp - rq;
-  if (!(a > 0.f)) return false;
-  const float a2 = a * a * 0.99999f;
-  const float sc = __fdiv_rn(256.f, a2);
-  if (!(sc < __int_as_float(0x7f800000))) return false;
-  constexpr int NS = P > 0 ? P / 32 : 1;
-  float d[NS];
-#pragma unroll
-  for (int j = 0; j < NS; ++j) {
-    d[j] = __int_as_float(0x7f800000);
-    if (j * 32 < np) {
-      const int e = j * 32 + lane;
-      if (e < np) {
-        const float4 p = pool[e];
-        d[j] = dist2_ref(qx, qy, qz, p.x, p.y, p.z);
-      }
-    }
-  }
-  // histogram of the distances within a, over 256 bins of [0, a2]
-  for (int b = lane; b < 256; b += 32) s.hist[b] = 0;
-  __syncwarp();
-#pragma unroll
-  for (int j = 0; j < NS; ++j)
-    if (d[j] <= a2) atomicAdd(&s.hist[min(255, __float2int_rz(__fmul_rz(d[j], sc)))], 1u);
-  __syncwarp();
-  uint32_t kk, nb, total;
-  const int bin = (int)hist_find(s.hist, (uint32_t)k, lane, &kk, &nb, &total);
-  stat_add<S>(s, lane, kStatCand, total);
-  if (total < (uint32_t)k || nb > 32) return false;
-  // the critical bin's entries (key, pool index) in sel / list
-  int pos = 0;
-#pragma unroll
-  for (int j = 0; j < NS; ++j) {
-    const bool in = d[j] <= a2 && min(255, __float2int_rz(__fmul_rz(d[j], sc))) == bin;
-    const unsigned bal = __ballot_sync(kFull, in);
-    if (in) {
-      const int o = pos + __popc(bal & lanemask_lt());
-      s.sel[o] = __float_as_uint(d[j]);
-      s.list[o] = (uint32_t)(j * 32 + lane);
-    }
-    pos += __popc(bal);
-  }
-  __syncwarp();
-  uint32_t kj = 0xffffffffu, oj = 0xffffffffu;
-  if (lane < (int)nb) {
-    kj = s.sel[lane];
-    oj = orig_index(m.pos4, __float_as_uint(pool[s.list[lane]].w));
-  }
-  uint32_t kth_oid;
-  const uint32_t kth_key = rank_critical(kj, oj, (int)nb, kk, lane, &kth_oid);
-  __syncwarp();  // the histogram is read: its words take the kept list
-  uint32_t* kkey = s.hist;
-  uint32_t* kid = s.hist + 128;
-  int nk = 0;
-#pragma unroll
-  for (int j = 0; j < NS; ++j) {
-    if (j * 32 < np) {
-      const uint32_t kb = __float_as_uint(d[j]);  // +inf past the pool: never kept
-      const int e = j * 32 + lane;
-      uint32_t sid = 0;
-      if (e < np) sid = __float_as_uint(pool[e].w);
-      bool kp = kb < kth_key;
-      if (kb == kth_key)
-        kp = kth_oid == 0xffffffffu || orig_index(m.pos4, sid) <= kth_oid;
-      const unsigned bal = __ballot_sync(kFull, kp);
-      const int o = nk + __popc(bal & lanemask_lt());
-      if (kp && o < kPoolMaxK) {
-        kkey[o] = kb;
-        kid[o] = sid;
-      }
-      nk += __popc(bal);
-    }
-  }
-  __syncwarp();
-  if (nk != k) return false;  // (the selection keeps exactly k)
-  stat_add<S>(s, lane, kStatQueries, 1);
-  stat_add<S>(s, lane, kStatPoolQueries, 1);
-  *maxd2 = __uint_as_float(kth_key);
-  return true;
-}
-
-// Output of one query from its kept photons (key[], id[] hold nk entries in
-// walk order; id = sorted positions, rewritten in place in knn mode).
-//   radiance: the estimate of integrator.h:141-150 into stage[0..3) when
-//             stage is set, else out.rgb[3 rec ..]
-//   knn:      the index list in the reference's order (photon_map.h:166-
-//             183), count and maxDist2 at row qi
-//   adjoint:  adj_in[3 rec ..] times d estimate / d throughput onto every
-//             kept photon of photon_adj
-// r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b} (radiance records).
-template <int MODE>
-__device__ __forceinline__ void emit(const MapDev& m, int lane, const uint32_t* key, uint32_t* id,
-                                     int nk, float maxd2, int k, float n_emitted,
-                                     const float4& r0, const float4& r1, const float4& r2,
-                                     int64_t qi, int64_t rec, const KnnOut& out, float* stage) {
-  if (MODE == kModeAdjoint) {
-    // d estimate / d throughput_i = f(wo, wi_i) / (n_emitted pi maxd2)
-    // for the kept photons (integrator.h:141-150)
-    const float ax = out.adj_in[3 * rec], ay = out.adj_in[3 * rec + 1],
-                az = out.adj_in[3 * rec + 2];
-    if (nk > 0 && (ax != 0.f || ay != 0.f || az != 0.f)) {
-      const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
-      const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
-      const float cr = __fdiv_rn(__fmul_rn(ax, __fdiv_rn(r0.w, kPI)), den);
-      const float cg = __fdiv_rn(__fmul_rn(ay, __fdiv_rn(r1.w, kPI)), den);
-      const float cb = __fdiv_rn(__fmul_rn(az, __fdiv_rn(r2.w, kPI)), den);
-      for (int i = lane; i < nk; i += 32) {
-        const uint32_t sid = id[i];
-        const float4 t = __ldg(m.thr4 + sid);
-        const float2 wv = __ldg(m.wi2 + sid);
-        const float cos_i = dot_ref(t.w, wv.x, wv.y, r2.x, r2.y, r2.z);
-        if (!(cos_o < 0.f) && !(cos_i < 0.f))
-          atomicAdd(out.photon_adj + orig_index(m.pos4, sid), make_float4(cr, cg, cb, 0.f));
-      }
-    }
-  } else if (MODE == kModeRadiance) {
-    const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
-    const float fr = __fdiv_rn(r0.w, kPI);
-    const float fg = __fdiv_rn(r1.w, kPI);
-    const float fb = __fdiv_rn(r2.w, kPI);
-    float lr = 0.f, lg = 0.f, lb = 0.f;
-    for (int i = lane; i < nk; i += 32) {
-      const uint32_t sid = id[i];
-      const float4 t = __ldg(m.thr4 + sid);
-      const float2 wv = __ldg(m.wi2 + sid);
-      const float cos_i = dot_ref(t.w, wv.x, wv.y, r2.x, r2.y, r2.z);
-      // Lambert::evaluate returns 0 when either cosine is < 0
-      if (!(cos_o < 0.f) && !(cos_i < 0.f)) {
-        lr = __fadd_rn(lr, __fmul_rn(fr, t.x));
-        lg = __fadd_rn(lg, __fmul_rn(fg, t.y));
-        lb = __fadd_rn(lb, __fmul_rn(fb, t.z));
-      }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      lr = __fadd_rn(lr, __shfl_xor_sync(kFull, lr, o));
-      lg = __fadd_rn(lg, __shfl_xor_sync(kFull, lg, o));
-      lb = __fadd_rn(lb, __shfl_xor_sync(kFull, lb, o));
-    }
-    if (lane == 0) {
-      float3 o3 = make_float3(0.f, 0.f, 0.f);
-      if (nk > 0) {
-        const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
-        o3 = make_float3(__fdiv_rn(lr, den), __fdiv_rn(lg, den), __fdiv_rn(lb, den));
-      }
-      float* dst = stage ? stage : out.rgb + 3 * rec;
-      dst[0] = o3.x;
-      dst[1] = o3.y;
-      dst[2] = o3.z;
-    }
-  } else {
-    for (int i = lane; i < nk; i += 32) id[i] = orig_index(m.pos4, id[i]);
     __syncwarp();
-    int32_t* orow = out.idx + qi * (int64_t)k;
-    for (int i = lane; i < nk; i += 32) {
-      const uint32_t ki = key[i], oi = id[i];
-      int rank = 0;
-      for (int j = 0; j < nk; ++j) {
-        const uint32_t kj = key[j], oj = id[j];
-        rank += (kj > ki) || (kj == ki && oj > oi);
-      }
-      orow[rank] = (int32_t)oi;
-    }
-    for (int r = nk + lane; r < k; r += 32) orow[r] = -1;
-    if (lane == 0) {
-      out.count[qi] = nk;
-      out.maxd2[qi] = maxd2;
-    }
-  }
-  __syncwarp();
-}
+    stat_add<S>(s, lane, kStatQueries, 1);
+    stat_add<S>(s, lane, kStatCand, (uint32_t)q.cnt);
+    const int cnt = q.cnt;
 
-// Answers queries [qb, qb + nw) (nw <= 32) on map m. Lane i loads the
-// record of query qb + i (record order[qb + i] when `order` is set). When
-// `stage` is set (radiance mode), query qb + i's radiance goes to
-// stage[3 i ..] instead of the output. P > 0: neighbourhood pools first
-// (when `pool` and k <= kPoolMaxK), the per-query search for the rest.
-template <int C, int P, int MODE, bool S>
-__device__ __forceinline__ void knn_window(const MapDev& m, const Levels& L, WarpBuf<C>& s,
-                                           int lane, const void* __restrict__ queries,
-                                           int64_t qb, int nw, int k, float n_emitted,
-                                           const KnnOut& out, const uint32_t* __restrict__ order,
-                                           int stride4, bool pool, float& r_hint,
-                                           float* stage) {
-  const float kInf = __int_as_float(0x7f800000);
-  float4 a0 = make_float4(0.f, 0.f, 0.f, 0.f), a1 = a0, a2 = a0;
-  int64_t rec = qb + lane;
-  if (lane < nw) {
-    if (MODE == kModeKnn) {
-      const float* q3 = reinterpret_cast<const float*>(queries) + 3 * rec;
-      a0 = make_float4(__ldcg(q3), __ldcg(q3 + 1), __ldcg(q3 + 2), 0.f);
+    // final selection
+    const bool all = cnt <= k;
+    uint32_t kth_key = 0, kth_oid = 0xffffffffu;
+    if (all) {
+      uint32_t mx = 0;
+      for (int i = lane; i < cnt; i += 32) mx = max(mx, s.key[i]);
+      kth_key = __reduce_max_sync(kFull, mx);
     } else {
-      if (order) rec = (int64_t)__ldg(order + qb + lane);
+      select_kth<C, S>(m.pos4, s, cnt, k, q.tau, lane, kth_key, kth_oid);
+    }
+    const int kept = all ? cnt : k;
+    const float maxd2 = kept > 0 ? __uint_as_float(kth_key) : 0.f;
+
+    if (MODE == kModeAdjoint) {
+      // d estimate / d throughput_i = f(wo, wi_i) / (n_emitted pi maxd2)
+      // for the kept photons (integrator.h:141-150)
       const float4* q4 = reinterpret_cast<const float4*>(queries) + stride4 * rec;
-      a0 = __ldcg(q4);
-      a1 = __ldcg(q4 + 1);
-      a2 = __ldcg(q4 + 2);
-    }
-  }
-  const bool mine = lane < nw;
-  const bool badq = mine && (m.n == 0 || isnan(a0.x) || isnan(a0.y) || isnan(a0.z));
-  unsigned fb = __ballot_sync(kFull, badq);  // answered by the per-query search
-  unsigned todo = __ballot_sync(kFull, mine) & ~fb;
-  Warm w;
-  w.have = false;
-  w.x = w.y = w.z = w.kth = 0.f;
-
-  auto emit_i = [&](int i, const uint32_t* key, uint32_t* id, int nk, float maxd2) {
-    float4 r0, r1, r2;
-    r0.x = __shfl_sync(kFull, a0.x, i); r0.y = __shfl_sync(kFull, a0.y, i);
-    r0.z = __shfl_sync(kFull, a0.z, i); r0.w = __shfl_sync(kFull, a0.w, i);
-    r1.x = __shfl_sync(kFull, a1.x, i); r1.y = __shfl_sync(kFull, a1.y, i);
-    r1.z = __shfl_sync(kFull, a1.z, i); r1.w = __shfl_sync(kFull, a1.w, i);
-    r2.x = __shfl_sync(kFull, a2.x, i); r2.y = __shfl_sync(kFull, a2.y, i);
-    r2.z = __shfl_sync(kFull, a2.z, i); r2.w = __shfl_sync(kFull, a2.w, i);
-    const int64_t ri = __shfl_sync(kFull, rec, i);
-    emit<MODE>(m, lane, key, id, nk, maxd2, k, n_emitted, r0, r1, r2, qb + i, ri, out,
-               stage ? stage + 3 * i : nullptr);
-  };
-  auto answer = [&](int i) {  // the per-query search
-    const float qx = __shfl_sync(kFull, a0.x, i), qy = __shfl_sync(kFull, a0.y, i),
-                qz = __shfl_sync(kFull, a0.z, i);
-    float maxd2;
-    const int nk = search_one<C, S>(m, L, s, lane, qx, qy, qz, k, w, r_hint, &maxd2);
-    emit_i(i, s.key, s.id, nk, maxd2);
-  };
-
-  if constexpr (P > 0) {
-   if (pool && k <= kPoolMaxK && m.nlevels > 1) {
-    if (!(r_hint > 0.f) && todo) {  // a warp without a k-th distance yet
-      const int i = __ffs(todo) - 1;
-      todo &= todo - 1;
-      answer(i);
-    }
-    while (todo && r_hint > 0.f) {
-      const int lead = __ffs(todo) - 1;
-      const float lx = __shfl_sync(kFull, a0.x, lead), ly = __shfl_sync(kFull, a0.y, lead),
-                  lz = __shfl_sync(kFull, a0.z, lead);
-      const float gr = kPoolGroup * r_hint;
-      const bool mem = lane == lead || (((todo >> lane) & 1u) &&
-                                        dist2_ref(a0.x, a0.y, a0.z, lx, ly, lz) <= gr * gr);
-      const unsigned mset = __ballot_sync(kFull, mem);
-      todo &= ~mset;
-      // centre: the middle of the members' bounding box
-      float lo_x = mem ? a0.x : kInf, lo_y = mem ? a0.y : kInf, lo_z = mem ? a0.z : kInf;
-      float hi_x = mem ? a0.x : -kInf, hi_y = mem ? a0.y : -kInf, hi_z = mem ? a0.z : -kInf;
+      const float4 r0 = HIO ? s.rec[buf][0] : __ldg(q4);
+      const float4 r1 = HIO ? s.rec[buf][1] : __ldg(q4 + 1);
+      const float4 r2 = HIO ? s.rec[buf][2] : __ldg(q4 + 2);
+      const float ax = out.adj_in[3 * rec], ay = out.adj_in[3 * rec + 1],
+                  az = out.adj_in[3 * rec + 2];
+      const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
+      if (kept > 0 && (ax != 0.f || ay != 0.f || az != 0.f)) {
+        const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
+        const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
+        const float cr = __fdiv_rn(__fmul_rn(ax, __fdiv_rn(r0.w, kPI)), den);
+        const float cg = __fdiv_rn(__fmul_rn(ay, __fdiv_rn(r1.w, kPI)), den);
+        const float cb = __fdiv_rn(__fmul_rn(az, __fdiv_rn(r2.w, kPI)), den);
+        for (int i = lane; i < nk; i += 32) {
+          const uint32_t id = s.id[i];
+          const float4 t = __ldg(m.thr4 + id);
+          const float2 w = __ldg(m.wi2 + id);
+          const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
+          if (!(cos_o < 0.f) && !(cos_i < 0.f))
+            atomicAdd(out.photon_adj + orig_index(m.pos4, id), make_float4(cr, cg, cb, 0.f));
+        }
+      }
+    } else if (MODE == kModeRadiance) {
+      // r0 = {pos, rho.r}, r1 = {wo, rho.g}, r2 = {ns, rho.b}
+      const float4* q4 = reinterpret_cast<const float4*>(queries) + stride4 * rec;
+      const float4 r0 = HIO ? s.rec[buf][0] : __ldg(q4);
+      const float4 r1 = HIO ? s.rec[buf][1] : __ldg(q4 + 1);
+      const float4 r2 = HIO ? s.rec[buf][2] : __ldg(q4 + 2);
+      const float cos_o = dot_ref(r1.x, r1.y, r1.z, r2.x, r2.y, r2.z);
+      const float fr = __fdiv_rn(r0.w, kPI);
+      const float fg = __fdiv_rn(r1.w, kPI);
+      const float fb = __fdiv_rn(r2.w, kPI);
+      // the kept entries, in the walk's order whatever the bound was, so
+      // the sum below does not depend on the order queries are answered
+      const int nk = all ? cnt : compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
+      float lr = 0.f, lg = 0.f, lb = 0.f;
+      for (int i = lane; i < nk; i += 32) {
+        const uint32_t id = s.id[i];
+        {
+          const float4 t = __ldg(m.thr4 + id);
+          const float2 w = __ldg(m.wi2 + id);
+          const float cos_i = dot_ref(t.w, w.x, w.y, r2.x, r2.y, r2.z);
+          // Lambert::evaluate returns 0 when either cosine is < 0
+          if (!(cos_o < 0.f) && !(cos_i < 0.f)) {
+            lr = __fadd_rn(lr, __fmul_rn(fr, t.x));
+            lg = __fadd_rn(lg, __fmul_rn(fg, t.y));
+            lb = __fadd_rn(lb, __fmul_rn(fb, t.z));
+          }
+        }
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
-        lo_x = fminf(lo_x, __shfl_xor_sync(kFull, lo_x, o));
-        lo_y = fminf(lo_y, __shfl_xor_sync(kFull, lo_y, o));
-        lo_z = fminf(lo_z, __shfl_xor_sync(kFull, lo_z, o));
-        hi_x = fmaxf(hi_x, __shfl_xor_sync(kFull, hi_x, o));
-        hi_y = fmaxf(hi_y, __shfl_xor_sync(kFull, hi_y, o));
-        hi_z = fmaxf(hi_z, __shfl_xor_sync(kFull, hi_z, o));
+        lr = __fadd_rn(lr, __shfl_xor_sync(kFull, lr, o));
+        lg = __fadd_rn(lg, __shfl_xor_sync(kFull, lg, o));
+        lb = __fadd_rn(lb, __shfl_xor_sync(kFull, lb, o));
       }
-      Query pq;
-      pq.x = 0.5f * (lo_x + hi_x);
-      pq.y = 0.5f * (lo_y + hi_y);
-      pq.z = 0.5f * (lo_z + hi_z);
-      const float rc2 = mem ? dist2_ref(a0.x, a0.y, a0.z, pq.x, pq.y, pq.z) : 0.f;
-      const float rc = sqrtf(__uint_as_float(__reduce_max_sync(kFull, __float_as_uint(rc2))));
-      const float R = (kPoolFactor * r_hint + rc) * 1.00002f;
-      pq.tau = R * R;
-      pq.k = k;
-      pq.cnt = 0;
-      collect<C, P, S>(m, L, pq, s, lane);
-      const int np = pq.cnt;
-      if (np > P) {
-        fb |= mset;
-        continue;
-      }
-      const float rp = sqrtf(pq.tau) * 0.99999f;
-      unsigned mm = mset;
-      while (mm) {
-        const int i = __ffs(mm) - 1;
-        mm &= mm - 1;
-        const float qx = __shfl_sync(kFull, a0.x, i), qy = __shfl_sync(kFull, a0.y, i),
-                    qz = __shfl_sync(kFull, a0.z, i);
-        float maxd2;
-        if (pool_query<C, P, S>(m, s, lane, np, qx, qy, qz, pq.x, pq.y, pq.z, rp, k, &maxd2)) {
-          emit_i(i, s.hist, s.hist + 128, k, maxd2);
-          r_hint = sqrtf(maxd2);
+      if (lane == 0) {
+        float3 o3 = make_float3(0.f, 0.f, 0.f);
+        if (kept > 0) {
+          const float den = __fmul_rn(__fmul_rn(n_emitted, kPI), maxd2);
+          o3 = make_float3(__fdiv_rn(lr, den), __fdiv_rn(lg, den),
+                           __fdiv_rn(lb, den));
+        }
+        if (HIO && !order) {
+          float* r = reinterpret_cast<float*>(s.id + C - kStageWords) + 3 * (qi & 7);
+          r[0] = o3.x; r[1] = o3.y; r[2] = o3.z;
         } else {
-          fb |= 1u << i;
+          out.rgb[3 * rec + 0] = o3.x;
+          out.rgb[3 * rec + 1] = o3.y;
+          out.rgb[3 * rec + 2] = o3.z;
         }
       }
-    }
-   }
-  }
-  fb |= todo;
-  // the per-query search for the rest, in query order
-  while (fb) {
-    const int i = __ffs(fb) - 1;
-    fb &= fb - 1;
-    answer(i);
-  }
-}
-
-// Answers the work item [qb, qe) in windows of up to 32 queries; in
-// radiance mode without `order` the radiance of the item (at most kChunk
-// queries, qb a multiple of 8) is staged and stored together (16-byte
-// words when the output allows: few, wide stores into mapped host memory).
-template <int C, int P, int MODE, bool S>
-__device__ __forceinline__ void knn_item(const MapDev& m, const Levels& L, WarpBuf<C>& s,
-                                         int lane, const void* __restrict__ queries, int64_t qb,
-                                         int64_t qe, int k, float n_emitted, const KnnOut& out,
-                                         const uint32_t* __restrict__ order, int stride4,
-                                         bool pool, float& r_hint) {
-  const bool staged = MODE == kModeRadiance && !order && qe - qb <= kChunk;
-  for (int64_t wb = qb; wb < qe; wb += 32) {
-    const int nw = (int)min((int64_t)32, qe - wb);
-    knn_window<C, P, MODE, S>(m, L, s, lane, queries, wb, nw, k, n_emitted, out, order, stride4,
-                              pool, r_hint, staged ? s.stage : nullptr);
-  }
-  if (staged) {
-    __syncwarp();
-    const int nf = 3 * (int)(qe - qb);
-    float* dst = out.rgb + 3 * qb;
-    if (nf % 4 == 0 && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
-      if (lane < nf / 4)
-        reinterpret_cast<float4*>(dst)[lane] = reinterpret_cast<const float4*>(s.stage)[lane];
+      // work items without `order` start at multiples of 8: a group of 8 is
+      // complete at qi % 8 == 7 or cut by the end of the queries
+      if (HIO && !order && ((qi & 7) == 7 || qi + 1 == qe)) {
+        __syncwarp();
+        const int64_t g0 = qi & ~(int64_t)7;
+        const int nf = 3 * (int)(qi + 1 - g0);
+        float* dst = out.rgb + 3 * g0;
+        const float* src = reinterpret_cast<const float*>(s.id + C - kStageWords);
+        if (nf == kStageWords && (reinterpret_cast<uintptr_t>(dst) & 15) == 0) {
+          if (lane < kStageWords / 4)
+            reinterpret_cast<float4*>(dst)[lane] = reinterpret_cast<const float4*>(src)[lane];
+        } else if (lane < nf) {
+          dst[lane] = src[lane];
+        }
+      }
     } else {
-      for (int i = lane; i < nf; i += 32) dst[i] = s.stage[i];
+      int n2 = cnt;
+      if (!all) n2 = compact_kept(m.pos4, s, cnt, kth_key, kth_oid, lane);
+      for (int i = lane; i < n2; i += 32)
+        s.id[i] = orig_index(m.pos4, s.id[i]);
+      __syncwarp();
+      int32_t* orow = out.idx + qi * (int64_t)k;
+      for (int i = lane; i < n2; i += 32) {
+        const uint32_t ki = s.key[i], oi = s.id[i];
+        int rank = 0;
+        for (int j = 0; j < n2; ++j) {
+          const uint32_t kj = s.key[j], oj = s.id[j];
+          rank += (kj > ki) || (kj == ki && oj > oi);
+        }
+        orow[rank] = (int32_t)oi;
+      }
+      for (int r = n2 + lane; r < k; r += 32) orow[r] = -1;
+      if (lane == 0) {
+        out.count[qi] = n2;
+        out.maxd2[qi] = maxd2;
+      }
     }
     __syncwarp();
+
+    if (!bad && kept >= k) {
+      have_prev = true;
+      pqx = q.x; pqy = q.y; pqz = q.z;
+      pkth = maxd2;
+      r_hint = sqrtf(maxd2);
+    } else {
+      have_prev = false;
+    }
   }
 }
 
-// Threads per block and minimum resident blocks of a kernel with search
-// buffer C and pool P.
-constexpr int knn_threads(int C, int P) { return P > 0 ? 128 : (C <= 512 ? 256 : 128); }
-constexpr int knn_min_blocks(int C, int P) { return P > 0 ? 5 : (C <= 512 ? 4 : 2); }
+// The tree shape and the cell grid's description of map m (one thread):
+// the grid is used when `grid` is set and the map has one.
+__device__ __forceinline__ void load_levels(const MapDev& m, Levels& L, bool grid) {
+#pragma unroll
+  for (int i = 0; i < kMaxLevels; ++i)  // constant indices: m stays in
+    L.oc[i] = make_int2(m.lvl_off[i], m.lvl_cnt[i]);  // the parameter bank
+  L.glmax = grid && m.grid ? m.grid_lmax : 0;
+#pragma unroll
+  for (int i = 0; i < kGridLevels; ++i) L.goff[i] = m.grid_off[i];
+  float mn = __int_as_float(0x7f800000);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    // the box as the build's morton_kernel reads it
+    const float lo = L.glmax ? from_ordered(m.grid[a]) : 0.f;
+    const float ext = L.glmax ? from_ordered(m.grid[3 + a]) - lo : 0.f;
+    L.glo[a] = lo;
+    L.gext[a] = ext;
+    if (ext > 0.f) mn = fminf(mn, ext);
+  }
+  L.gmin_ext = mn < __int_as_float(0x7f800000) ? mn : 0.f;
+}
 
-template <int C, int P, int MODE, bool S>
-__global__ void __launch_bounds__(knn_threads(C, P), knn_min_blocks(C, P))
+template <int C, int MODE, bool S>
+__global__ void __launch_bounds__(256, 4)
     knn_kernel(MapDev m, const void* __restrict__ queries, int64_t nq, int k,
                float n_emitted, KnnOut out,
                unsigned long long* __restrict__ counter,
                const uint32_t* __restrict__ order, int stride4, int64_t head_items,
-               int pool) {
+               int grid) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ Levels L;
   WarpBuf<C>& s = reinterpret_cast<WarpBuf<C>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int i = 0; i < kMaxLevels; ++i) {  // constant indices: m stays in
-      L.oc[i] = make_int2(m.lvl_off[i], m.lvl_cnt[i]);  // the parameter bank
-    }
-  }
+  if (threadIdx.x == 0) load_levels(m, L, grid != 0);
   if (lane < 8) s.stat[lane] = 0;
   __syncthreads();
   float r_hint = -1.f;  // last exact k-th distance this warp found
@@ -1314,8 +1324,8 @@ __global__ void __launch_bounds__(knn_threads(C, P), knn_min_blocks(C, P))
     if (qb >= nq) break;
     const int64_t qe = min(nq, qb + (head ? kChunk : kTail));
 
-    knn_item<C, P, MODE, S>(m, L, s, lane, queries, qb, qe, k, n_emitted, out, order, stride4,
-                            pool != 0, r_hint);
+    knn_chunk<C, MODE, S, true>(m, L, s, lane, queries, qb, qe, k, n_emitted, out, order, stride4,
+                          r_hint);
     if (S) {
       __syncwarp();
       if (lane < kNumStats) {
@@ -1327,15 +1337,15 @@ __global__ void __launch_bounds__(knn_threads(C, P), knn_min_blocks(C, P))
   }
 }
 
-template <int C, int P, int MODE>
+template <int C, int MODE>
 static cudaError_t launch_one(const MapDev& m, const void* queries,
                               int64_t nq, int k, float n_emitted, KnnOut out,
                               unsigned long long* counter, int num_sms,
                               cudaStream_t st, const uint32_t* order,
-                              int stride4, bool pool) {
-  constexpr int kThreads = knn_threads(C, P);
+                              int stride4, bool grid) {
+  constexpr int kThreads = (C <= 512) ? 256 : 128;
   const size_t smem = (kThreads / 32) * sizeof(WarpBuf<C>);
-  auto kern = out.stats ? knn_kernel<C, P, MODE, true> : knn_kernel<C, P, MODE, false>;
+  auto kern = out.stats ? knn_kernel<C, MODE, true> : knn_kernel<C, MODE, false>;
   cudaError_t e = cudaFuncSetAttribute(
       kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
@@ -1356,7 +1366,7 @@ static cudaError_t launch_one(const MapDev& m, const void* queries,
   if (e != cudaSuccess) return e;
   kern<<<(unsigned)blocks, kThreads, smem, st>>>(m, queries, nq, k, n_emitted,
                                                  out, counter, order, stride4, head_items,
-                                                 pool ? 1 : 0);
+                                                 grid ? 1 : 0);
   return cudaGetLastError();
 }
 
@@ -1364,30 +1374,27 @@ template <int MODE>
 static cudaError_t launch_mode(const MapDev& m, const void* queries, int64_t nq, int k,
                                float n_emitted, KnnOut out, unsigned long long* counter,
                                int num_sms, cudaStream_t st, const uint32_t* order, int stride4,
-                               bool pool) {
-  if (k <= kPoolMaxK)
-    return launch_one<kPoolBuf, kPoolSize, MODE>(m, queries, nq, k, n_emitted, out, counter,
-                                                 num_sms, st, order, stride4, pool);
+                               bool grid) {
   if (k <= 224)
-    return launch_one<512, 0, MODE>(m, queries, nq, k, n_emitted, out, counter, num_sms, st,
-                                    order, stride4, false);
-  return launch_one<2048, 0, MODE>(m, queries, nq, k, n_emitted, out, counter, num_sms, st,
-                                   order, stride4, false);
+    return launch_one<512, MODE>(m, queries, nq, k, n_emitted, out, counter, num_sms, st, order,
+                                 stride4, grid);
+  return launch_one<2048, MODE>(m, queries, nq, k, n_emitted, out, counter, num_sms, st, order,
+                                stride4, grid);
 }
 
 cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                        int k, int mode, float n_emitted, KnnOut out,
                        unsigned long long* counter, int num_sms,
-                       cudaStream_t st, const uint32_t* order, int stride4, bool pool) {
+                       cudaStream_t st, const uint32_t* order, int stride4, bool grid) {
   if (nq <= 0) return cudaSuccess;
   if (mode == kModeAdjoint)
     return launch_mode<kModeAdjoint>(m, queries, nq, k, n_emitted, out, counter, num_sms, st,
-                                     order, stride4, pool);
+                                     order, stride4, grid);
   if (mode == kModeRadiance)
     return launch_mode<kModeRadiance>(m, queries, nq, k, n_emitted, out, counter, num_sms, st,
-                                      order, stride4, pool);
+                                      order, stride4, grid);
   return launch_mode<kModeKnn>(m, queries, nq, k, n_emitted, out, counter, num_sms, st, order,
-                               stride4, pool);
+                               stride4, grid);
 }
 
 }  // namespace pm
@@ -1399,11 +1406,9 @@ namespace pm {
 // persistent launch. A work item is `chunk` consecutive queries of one
 // scene (in the order of the sorted keys: scene, then Morton code); a warp
 // takes items from `counter` until none are left, switching its copy of the
-// photon map (map pointers, tree shape) when the scene changes. The
-// kernel with search buffer kPoolBuf pools neighbourhoods for scenes with
-// k <= kPoolMaxK.
-template <int C, int P>
-__global__ void __launch_bounds__(256, 2)
+// photon map (map pointers, tree shape) when the scene changes.
+template <int C>
+__global__ void __launch_bounds__(256, 4)
     knn_batch_kernel(BatchTables t, const float4* __restrict__ slots,
                      const uint32_t* __restrict__ order, const int64_t* __restrict__ qoff,
                      const int64_t* __restrict__ item_off, int chunk, KnnOut out,
@@ -1431,9 +1436,7 @@ __global__ void __launch_bounds__(256, 2)
       if (lane == 0) {
         const BatchScene& bs = t.scenes[sc];
         wmap[warp] = bs.map;
-        for (int i = 0; i < kMaxLevels; ++i) {
-          wlev[warp].oc[i] = make_int2(bs.map.lvl_off[i], bs.map.lvl_cnt[i]);
-        }
+        load_levels(bs.map, wlev[warp], true);
       }
       __syncwarp();
       cur = sc;
@@ -1443,32 +1446,23 @@ __global__ void __launch_bounds__(256, 2)
     }
     const int64_t qb = qoff[sc] + ((int64_t)c0 - ioff[sc]) * chunk;
     const int64_t qe = min(qoff[sc + 1], qb + chunk);
-    knn_item<C, P, kModeRadiance, false>(wmap[warp], wlev[warp], s, lane, slots, qb, qe, k,
-                                         n_emitted, out, order, 4, true, r_hint);
+    knn_chunk<C, kModeRadiance, false, false>(wmap[warp], wlev[warp], s, lane, slots, qb, qe, k,
+                                       n_emitted, out, order, 4, r_hint);
   }
-}
-
-// The kernel behind a tuning's candidate-buffer size: 512 selects the
-// pooling kernel (search buffer kPoolBuf), 2048 the large-k one.
-template <class F>
-static cudaError_t with_batch_kernel(int buffer, F f) {
-  if (buffer <= 512) return f(knn_batch_kernel<kPoolBuf, kPoolSize>, sizeof(WarpBuf<kPoolBuf>));
-  return f(knn_batch_kernel<2048, 0>, sizeof(WarpBuf<2048>));
 }
 
 cudaError_t batch_knn_prepare(int warps, int buffer, int* blocks_per_sm) {
   if (warps < 1 || warps > 8) return cudaErrorInvalidValue;
-  return with_batch_kernel(buffer, [&](auto kern, size_t wb) {
-    const size_t smem = (size_t)warps * wb;
-    cudaError_t e =
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, smem);
-    if (e != cudaSuccess) return e;
-    *blocks_per_sm = per_sm < 1 ? 1 : per_sm;
-    return cudaSuccess;
-  });
+  auto kern = buffer <= 512 ? knn_batch_kernel<512> : knn_batch_kernel<2048>;
+  const size_t smem =
+      (size_t)warps * (buffer <= 512 ? sizeof(WarpBuf<512>) : sizeof(WarpBuf<2048>));
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  int per_sm = 0;
+  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 32 * warps, smem);
+  if (e != cudaSuccess) return e;
+  *blocks_per_sm = per_sm < 1 ? 1 : per_sm;
+  return cudaSuccess;
 }
 
 cudaError_t batch_knn_launch(const BatchTables& t, const float4* slots, const uint32_t* order,
@@ -1477,6 +1471,9 @@ cudaError_t batch_knn_launch(const BatchTables& t, const float4* slots, const ui
                              unsigned long long* counter, int num_sms, cudaStream_t st) {
   if (warps < 1 || warps > 8 || chunk < 1) return cudaErrorInvalidValue;
   const int threads = 32 * warps;
+  auto kern = buffer <= 512 ? knn_batch_kernel<512> : knn_batch_kernel<2048>;
+  const size_t smem =
+      (size_t)warps * (buffer <= 512 ? sizeof(WarpBuf<512>) : sizeof(WarpBuf<2048>));
   int64_t blocks = (int64_t)num_sms * blocks_per_sm;
   const int64_t need = (max_items + warps - 1) / warps;
   if (blocks > need) blocks = need;
@@ -1485,12 +1482,9 @@ cudaError_t batch_knn_launch(const BatchTables& t, const float4* slots, const ui
   if (e != cudaSuccess) return e;
   KnnOut out{};
   out.rgb = res;
-  return with_batch_kernel(buffer, [&](auto kern, size_t wb) {
-    const size_t smem = (size_t)warps * wb;
-    kern<<<(unsigned)blocks, threads, smem, st>>>(t, slots, order, qoff, item_off, chunk, out,
-                                                  counter);
-    return cudaGetLastError();
-  });
+  kern<<<(unsigned)blocks, threads, smem, st>>>(t, slots, order, qoff, item_off, chunk, out,
+                                                counter);
+  return cudaGetLastError();
 }
 
 }  // namespace pm

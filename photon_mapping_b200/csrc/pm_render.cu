@@ -76,8 +76,9 @@ __device__ V3 direct_light(const SceneDev& sc, const Surf& s, V3 wo,
 template <bool D, int STACK>
 __device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
                        const Material* m, V3 w, Rng& rng, int64_t base,
-                       int& nq, int pid_w) {
+                       int& nq, int pid_w, unsigned& nr) {
   for (int depth = 0; depth < a.max_depth; ++depth) {
+    ++nr;
     V3 wi_l;
     float pdf;
     const V3 f = bxdf_sample(*m, world_to_local(wo, s.dpdu, s.ns, s.dpdv),
@@ -102,7 +103,8 @@ __device__ void gather(const RenderArgs& a, const SceneDev& sc, Surf s, V3 wo,
 
 // One pixel's samples of the camera pass (all a.batch of them).
 template <bool D, int STACK>
-__device__ __forceinline__ void camera_pixel(const SceneDev& sc, const RenderArgs& a, int p) {
+__device__ __forceinline__ void camera_pixel(const SceneDev& sc, const RenderArgs& a, int p,
+                                             unsigned& nr) {
   const int i = p / a.width, j = p % a.width;
   Rng rng{a.rng_state[p]};
   for (int sidx = 0; sidx < a.batch; ++sidx) {
@@ -132,6 +134,7 @@ __device__ __forceinline__ void camera_pixel(const SceneDev& sc, const RenderArg
       const Frame f = st[--sp];
       if (f.depth >= a.max_depth) continue;
       Hit h;
+      ++nr;
       if (!intersect_t<STACK>(sc, f.o, f.d, kRayEps, __int_as_float(0x7f7fffff), h)) continue;
       const Surf s = surface_at(sc, f.o, f.d, h);
       const Material& m = sc.mat[h.prim];
@@ -145,6 +148,7 @@ __device__ __forceinline__ void camera_pixel(const SceneDev& sc, const RenderArg
         if (f.depth >= a.fg_depth) {
           emit_query<D>(a, base, nq, kQueryGlobal, s, wo, mat_rho(m), f.w, -1, pid);
         } else {
+          ++nr;  // the shadow ray
           const V3 ld = f.w * direct_light<STACK>(sc, s, wo, m, rng);
           direct = direct + ld;
           if (D && nn < a.q_per_sample)
@@ -152,7 +156,7 @@ __device__ __forceinline__ void camera_pixel(const SceneDev& sc, const RenderArg
           emit_query<D>(a, base, nq, kQueryCaustics, s, wo, mat_rho(m), f.w, -1, pid);
           const V3 wg = f.w * a.inv_gather;
           for (int g = 0; g < a.n_gather; ++g)
-            gather<D, STACK>(a, sc, s, wo, &m, wg, rng, base, nq, pid);
+            gather<D, STACK>(a, sc, s, wo, &m, wg, rng, base, nq, pid, nr);
         }
         continue;
       }
@@ -210,8 +214,12 @@ template <bool D>
 __global__ void __launch_bounds__(128)
     camera_kernel(SceneDev sc, RenderArgs a) {
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= a.width * a.height) return;
-  camera_pixel<D, kBvhStack>(sc, a, p);
+  unsigned nr = 0;
+  if (p < a.width * a.height) camera_pixel<D, kBvhStack>(sc, a, p, nr);
+  if (a.rays) {
+    const unsigned tot = __reduce_add_sync(kFull, nr);
+    if ((threadIdx.x & 31) == 0 && tot) atomicAdd(a.rays, (unsigned long long)tot);
+  }
 }
 
 __global__ void rng_init_kernel(unsigned long long* st, int w, int n) {
@@ -499,7 +507,8 @@ __global__ void __launch_bounds__(256)
   const int p = (int)(g - off[s]);
   const int i = p / bs.ra.width, j = p % bs.ra.width;
   bs.ra.rng_state[p] = (unsigned long long)(j + bs.ra.width * i);  // UniformSampler(j + w*i)
-  camera_pixel<false, STACK>(bs.sc, bs.ra, p);
+  unsigned nr = 0;
+  camera_pixel<false, STACK>(bs.sc, bs.ra, p, nr);
 }
 
 void batch_camera_launch(const BatchTables& t, int64_t total_pix, int block, int stack,

@@ -30,6 +30,7 @@ struct RenderArgs {
   float4* nee;          // per sample, q_per_sample records {next-event
                         // radiance, parameter of the surface (int bits)}
   int* nee_count;       // per sample
+  unsigned long long* rays;  // closest-hit queries of the pass (added to), or null
 };
 
 struct PathArgs {

@@ -100,7 +100,7 @@ __device__ __forceinline__ void photon_emit(const SceneDev& sc, const TraceArgs&
 // :497-557 caustics); false when the path ends.
 template <int MODE, int STACK>
 __device__ __forceinline__ bool photon_step(const SceneDev& sc, const TraceArgs& a,
-                                            PhotonPath& p, ReplaySmem* rs) {
+                                            PhotonPath& p, ReplaySmem* rs, unsigned& nrays) {
   if (p.k >= a.max_depth) return false;
   const V3 dec = MODE != kTracePlain ? p.td : p.thr;
   if (has_nan(dec)) {
@@ -112,6 +112,7 @@ __device__ __forceinline__ bool photon_step(const SceneDev& sc, const TraceArgs&
     return false;
   }
   Hit h;
+  ++nrays;
   if (!intersect_t<STACK>(sc, p.org, p.dir, kRayEps, __int_as_float(0x7f7fffff), h))
     return false;  // photon goes to the sky
   const Surf s = surface_at(sc, p.org, p.dir, h);
@@ -199,6 +200,7 @@ __device__ __forceinline__ void trace_persistent(unsigned long long* next, long 
   PhotonPath p;
   int src = 0;
   bool live = false, done = false;
+  unsigned nrays = 0;  // closest-hit queries of this thread
   while (true) {
     const unsigned want = __ballot_sync(kFull, !live && !done);
     if (want) {
@@ -220,7 +222,12 @@ __device__ __forceinline__ void trace_persistent(unsigned long long* next, long 
       }
     }
     if (__ballot_sync(kFull, live) == 0) break;
-    if (live) live = photon_step<MODE, STACK>(scene(src), args(src), p, rs);
+    if (live) live = photon_step<MODE, STACK>(scene(src), args(src), p, rs, nrays);
+  }
+  unsigned long long* rays = args(0).rays;
+  if (rays) {
+    const unsigned tot = __reduce_add_sync(kFull, nrays);
+    if (lane == 0) atomicAdd(rays, (unsigned long long)tot);
   }
 }
 

@@ -19,6 +19,7 @@ struct TraceArgs {
   unsigned long long cap;       // capacity of out / keys
   unsigned* status;  // [0] NaN throughput, [1] negative throughput
   unsigned long long* next;  // work counter of the persistent kernel (reset by the launch)
+  unsigned long long* rays;  // closest-hit queries traced (added to), or null
   // Differentiable render; all null in a plain trace.
   //   dmat != null: Russian roulette and the NaN / negative stops are
   //     decided on a second throughput carried with these materials, so the

@@ -27,12 +27,14 @@ class RenderStats(C.Structure):
     _fields_ = [("samples", C.c_int64), ("dropped_nan", C.c_int64),
                 ("dropped_negative", C.c_int64), ("queries_global", C.c_int64),
                 ("queries_caustics", C.c_int64), ("passes", C.c_int32), ("reserved", C.c_int32),
-                ("accum_rel_err", C.c_double)]
+                ("accum_rel_err", C.c_double), ("rays", C.c_int64), ("camera_ms", C.c_float),
+                ("estimate_ms", C.c_float)]
 
     def as_dict(self) -> dict:
-        d = {k: int(getattr(self, k)) for k, _ in self._fields_
-             if k not in ("reserved", "accum_rel_err")}
-        d["accum_rel_err"] = float(self.accum_rel_err)
+        d = {k: int(getattr(self, k)) for k, t in self._fields_
+             if k != "reserved" and t not in (C.c_float, C.c_double)}
+        for k in ("accum_rel_err", "camera_ms", "estimate_ms"):
+            d[k] = float(getattr(self, k))
         return d
 
 
@@ -44,10 +46,11 @@ class IntegrateParams(C.Structure):
 
 class TraceStats(C.Structure):
     _fields_ = [("emitted", C.c_int64), ("stored", C.c_int64),
-                ("nan_throughput", C.c_uint32), ("negative_throughput", C.c_uint32)]
+                ("nan_throughput", C.c_uint32), ("negative_throughput", C.c_uint32),
+                ("rays", C.c_int64), ("trace_ms", C.c_float), ("build_ms", C.c_float)]
 
     def as_dict(self) -> dict:
-        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+        return {k: (float if t is C.c_float else int)(getattr(self, k)) for k, t in self._fields_}
 
 
 def trace_photons(ctx: Context, map_id: int, seed: int, n_emit: int, max_depth: int) -> dict:

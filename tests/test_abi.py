@@ -61,3 +61,26 @@ def test_status_strings_and_null_context(lib_path):
 def test_radiance_query_record_is_48_bytes():
     from photon_mapping_b200 import _native
     assert _native.RADIANCE_QUERY_FLOATS * 4 == 48
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """The ctypes mirrors of the statistics records have the C sizes and
+    field offsets of include/pm_cuda.h."""
+    import ctypes as C
+    from photon_mapping_b200 import _native as N
+    from photon_mapping_b200.integrator import RenderStats, TraceStats
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "pm_cuda.h"\n'
+                   'int main(void) {\n'
+                   '  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(pm_trace_stats),\n'
+                   '         offsetof(pm_trace_stats, rays), sizeof(pm_render_stats),\n'
+                   '         offsetof(pm_render_stats, rays), sizeof(pm_knn_stats),\n'
+                   '         offsetof(pm_knn_stats, grid_searches));\n'
+                   '  return 0;\n}\n')
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    assert got == [C.sizeof(TraceStats), TraceStats.rays.offset, C.sizeof(RenderStats),
+                   RenderStats.rays.offset, 8 * len(N.Context.STAT_FIELDS),
+                   8 * N.Context.STAT_FIELDS.index("grid_searches")]
