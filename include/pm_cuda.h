@@ -77,15 +77,11 @@ typedef struct pm_knn_stats {
   uint64_t queries;     /* queries answered                                  */
   uint64_t cold_starts; /* queries whose search radius was bounded afresh    */
   uint64_t candidates;  /* photons found within the search radius            */
-  uint64_t leaves;      /* 8-photon groups scanned (tree walks) and cell
-                           ranges scanned (grid searches)                    */
+  uint64_t leaves;      /* 8-photon groups scanned                           */
   uint64_t nodes;       /* inner tree nodes expanded                         */
   uint64_t selects;     /* k-th distance selections                          */
-  uint64_t walks;       /* candidate searches (tree walks and grid searches):
-                           more than one per query when a guessed radius
-                           held fewer than k photons                         */
-  uint64_t grid_searches; /* searches that listed their candidates from the
-                           map's cell grid instead of walking the tree       */
+  uint64_t walks;       /* tree walks: more than one per query when a guessed
+                           radius held fewer than k photons                  */
 } pm_knn_stats;
 
 /* Turns the kNN counters on (1) or off (0) for later launches. */
@@ -93,15 +89,6 @@ int pm_ctx_set_stats(pm_ctx* ctx, int enable);
 /* Copies the counters (waits for the context's stream); reset != 0 zeroes
  * them afterwards. */
 int pm_ctx_get_stats(pm_ctx* ctx, pm_knn_stats* out, int reset);
-
-/* Cell grids of the kNN searches (no reference counterpart; on by
- * default). pm_photonmap_build also files the sorted photons by cell of a
- * uniform grid (levels 3 to 7, 8^L cells, about 9.6 MB at 3M photons), and a
- * search whose radius suits a level lists its candidates from the cells
- * around the query instead of walking the box tree. 0 makes every search
- * walk the tree, 1 restores the grid. Results are identical either way;
- * only the speed changes. */
-int pm_ctx_set_knn_grid(pm_ctx* ctx, int enable);
 
 /* ---------------------------------------------------------- photon map */
 /* Replaces PhotonMap::setPhotons + PhotonMap::build

@@ -50,7 +50,6 @@ _SIGNATURES = {
     "pm_ctx_last_error": (C.c_char_p, [_vp]),
     "pm_status_string": (C.c_char_p, [C.c_int]),
     "pm_ctx_set_stats": (C.c_int, [_vp, C.c_int]),
-    "pm_ctx_set_knn_grid": (C.c_int, [_vp, C.c_int]),
     "pm_ctx_get_stats": (C.c_int, [_vp, _vp, C.c_int]),
     "pm_photonmap_build": (C.c_int, [_vp, C.c_int, _vp, _i64]),
     "pm_photonmap_build_device": (C.c_int, [_vp, C.c_int, _vp, _i64, _vp]),
@@ -158,17 +157,10 @@ class Context:
     def synchronize(self) -> None:
         self.check(self.lib.pm_ctx_synchronize(self.handle), "synchronize")
 
-    STAT_FIELDS = ("queries", "cold_starts", "candidates", "leaves", "nodes", "selects", "walks",
-                   "grid_searches")
+    STAT_FIELDS = ("queries", "cold_starts", "candidates", "leaves", "nodes", "selects", "walks")
 
     def set_stats(self, enable: bool) -> None:
         self.check(self.lib.pm_ctx_set_stats(self.handle, int(bool(enable))), "pm_ctx_set_stats")
-
-    def set_knn_grid(self, enable: bool) -> None:
-        """Cell-grid candidate lists in the kNN searches (on by default;
-        results are identical either way)."""
-        self.check(self.lib.pm_ctx_set_knn_grid(self.handle, int(bool(enable))),
-                   "pm_ctx_set_knn_grid")
 
     def get_stats(self, reset: bool = False) -> dict:
         buf = (C.c_uint64 * len(self.STAT_FIELDS))()

@@ -67,9 +67,6 @@ MapDev map_view(const DevMap& dm) {
     m.lvl_off[i] = i < dm.nlevels ? dm.lvl_off[i] : 0;
     m.lvl_cnt[i] = i < dm.nlevels ? dm.lvl_cnt[i] : 0;
   }
-  m.grid = dm.grid_lmax > 0 ? (const uint32_t*)dm.grid.ptr : nullptr;
-  m.grid_lmax = dm.grid_lmax;
-  for (int i = 0; i < kGridLevels; ++i) m.grid_off[i] = dm.grid_off[i];
   return m;
 }
 
@@ -85,7 +82,6 @@ int build_map(pm_ctx* c, DevMap& dm, const float* d_aos, int64_t n,
   c->diff.ready = false;
   dm.n = n;
   int total = map_levels(n, &dm.nlevels, dm.lvl_off, dm.lvl_cnt);
-  const size_t gw = grid_words(n, &dm.grid_lmax, dm.grid_off);
   if (n == 0) {
     dm.built = true;
     return PM_OK;
@@ -95,7 +91,6 @@ int build_map(pm_ctx* c, DevMap& dm, const float* d_aos, int64_t n,
       (st_ok = dm.thr4.ensure((size_t)n * sizeof(float4))) ||
       (st_ok = dm.wi2.ensure((size_t)n * sizeof(float2))) ||
       (st_ok = dm.boxes.ensure((size_t)total * 2 * sizeof(float4))) ||
-      (gw > 0 && (st_ok = dm.grid.ensure(gw * sizeof(uint32_t)))) ||
       (st_ok = c->scratch.ensure(map_build_scratch_bytes(n))))
     return set_err(c, st_ok, "photon map allocation (%lld photons)",
                    (long long)n);
@@ -108,7 +103,7 @@ int build_map(pm_ctx* c, DevMap& dm, const float* d_aos, int64_t n,
   map_build_launch((const float*)dm.aos.ptr, (int)n, (float4*)dm.pos4.ptr,
                    (float4*)dm.thr4.ptr, (float2*)dm.wi2.ptr,
                    (float4*)dm.boxes.ptr, dm.lvl_off, dm.lvl_cnt, dm.nlevels,
-                   c->scratch.ptr, st, (uint32_t*)dm.grid.ptr, dm.grid_lmax, dm.grid_off);
+                   c->scratch.ptr, st);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(c, e, "photon map build");
   dm.built = true;
@@ -208,13 +203,6 @@ int pm_ctx_set_stats(pm_ctx* c, int enable) {
     if (e != cudaSuccess) return cuda_status(c, e, "stats counters");
   }
   c->stats_on = enable != 0;
-  return PM_OK;
-}
-
-int pm_ctx_set_knn_grid(pm_ctx* c, int enable) {
-  PM_CHECK_CTX(c);
-  std::lock_guard<std::mutex> lk(c->mu);
-  c->knn_grid = enable != 0;
   return PM_OK;
 }
 
@@ -345,7 +333,7 @@ int pm_photonmap_knn(pm_ctx* c, int map, const float* queries, int64_t nq,
   o.count = m_cnt ? m_cnt : (int32_t*)((char*)c->q_out.ptr + ib);
   o.maxd2 = m_md2 ? m_md2 : (float*)((char*)c->q_out.ptr + ib + cb);
   e = knn_launch(map_view(dm), c->q_in.ptr, nq, k, kModeKnn, 0.f, o,
-                 c->next_counter(), c->num_sms, st, nullptr, 3, c->knn_grid);
+                 c->next_counter(), c->num_sms, st);
   if (e != cudaSuccess) return cuda_status(c, e, "knn launch");
   if ((!m_idx && (e = cudaMemcpyAsync(out_idx, o.idx, ib, cudaMemcpyDeviceToHost, st))) ||
       (!m_cnt && (e = cudaMemcpyAsync(out_count, o.count, cb, cudaMemcpyDeviceToHost, st))) ||
@@ -392,8 +380,7 @@ int pm_photonmap_radiance(pm_ctx* c, int map, const pm_radiance_query* q,
   o.stats = c->stats_ptr();
   o.rgb = mapped_out ? mapped_out : (float*)c->q_out.ptr;
   e = knn_launch(map_view(dm), d_q, nq, k, kModeRadiance,
-                 (float)n_emitted, o, c->next_counter(), c->num_sms, st, nullptr, 3,
-                 c->knn_grid);
+                 (float)n_emitted, o, c->next_counter(), c->num_sms, st);
   if (e != cudaSuccess) return cuda_status(c, e, "radiance launch");
   if (!mapped_out) {
     e = cudaMemcpyAsync(out_rgb, o.rgb, ob, cudaMemcpyDeviceToHost, st);
@@ -424,7 +411,7 @@ int pm_photonmap_radiance_device(pm_ctx* c, int map, const void* d_queries,
   o.rgb = (float*)d_out_rgb;
   cudaError_t e = knn_launch(map_view(dm), d_queries, nq, k, kModeRadiance,
                              (float)n_emitted, o, c->next_counter(),
-                             c->num_sms, as_stream(stream), nullptr, 3, c->knn_grid);
+                             c->num_sms, as_stream(stream));
   return cuda_status(c, e, "radiance launch");
 }
 

@@ -227,8 +227,7 @@ void enqueue_maps(pm_batch* b) {
                            (float*)dm.aos.ptr, b->scratch[i].ptr, b->side[i]);
       map_build_launch((const float*)dm.aos.ptr, m, (float4*)dm.pos4.ptr, (float4*)dm.thr4.ptr,
                        (float2*)dm.wi2.ptr, (float4*)dm.boxes.ptr, dm.lvl_off, dm.lvl_cnt,
-                       dm.nlevels, b->scratch[i].ptr, b->side[i], (uint32_t*)dm.grid.ptr,
-                       dm.grid_lmax, dm.grid_off);
+                       dm.nlevels, b->scratch[i].ptr, b->side[i]);
     }
   }
   for (int i = 0; i < ns; ++i) {
@@ -351,12 +350,10 @@ int plan(pm_batch* b) {
     const int64_t m = b->stored[i];
     dm.n = m;
     const int total = map_levels(m, &dm.nlevels, dm.lvl_off, dm.lvl_cnt);
-    const size_t gw = grid_words(m, &dm.grid_lmax, dm.grid_off);
     if (m > 0 &&
         ((s = dm.aos.ensure((size_t)m * 36)) || (s = dm.pos4.ensure((size_t)m * 16)) ||
          (s = dm.thr4.ensure((size_t)m * 16)) || (s = dm.wi2.ensure((size_t)m * 8)) ||
-         (s = dm.boxes.ensure((size_t)total * 32)) ||
-         (gw > 0 && (s = dm.grid.ensure(gw * 4)))))
+         (s = dm.boxes.ensure((size_t)total * 32))))
       return berr(b, s, "scene %d: photon map (%lld photons)", i, (long long)m);
     dm.built = true;
     const size_t sb = std::max(order_scratch_bytes(m), map_build_scratch_bytes(m));

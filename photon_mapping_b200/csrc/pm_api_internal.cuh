@@ -25,9 +25,7 @@ struct DevMap {
   int nlevels = 0;
   int lvl_off[kMaxLevels] = {};
   int lvl_cnt[kMaxLevels] = {};
-  int grid_lmax = 0;                  // cell grid: finest level (0: none)
-  int grid_off[kGridLevels] = {};
-  DevBuf aos, pos4, thr4, wi2, boxes, grid;
+  DevBuf aos, pos4, thr4, wi2, boxes;
   bool built = false;
   void release() {
     aos.release();
@@ -35,8 +33,6 @@ struct DevMap {
     thr4.release();
     wi2.release();
     boxes.release();
-    grid.release();
-    grid_lmax = 0;
     built = false;
     n = 0;
   }
@@ -127,7 +123,6 @@ struct pm_ctx {
   pm::DevBuf stats;        // pm_knn_stats counters (device)
   pm::DiffState diff;      // differentiable render
   bool stats_on = false;
-  bool knn_grid = true;    // cell-grid candidate lists in the kNN kernels
   unsigned long long* stats_ptr() {
     return stats_on ? (unsigned long long*)stats.ptr : nullptr;
   }

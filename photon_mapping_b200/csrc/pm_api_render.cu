@@ -64,8 +64,7 @@ int answer_queries(pm_ctx* c, const RenderArgs& a, int64_t ns, int64_t n_slots,
     o.photon_adj = slot_adj ? photon_adj[map] : nullptr;
     e = knn_launch(map_view(c->maps[map]), a.slots, nq, map == 0 ? kg : kc,
                    slot_adj ? kModeAdjoint : kModeRadiance, (float)c->map_emitted[map], o,
-                   c->next_counter(), c->num_sms, st, in_b ? vb : va, 4,
-                   c->knn_grid);
+                   c->next_counter(), c->num_sms, st, in_b ? vb : va, 4);
     if (e != cudaSuccess) return cuda_status(c, e, "render estimates");
   }
   return PM_OK;

@@ -20,14 +20,21 @@ constexpr float kPI = 3.14159265359f;
 // core.h:19
 constexpr float kRayEps = 1e-5f;
 
+// Lane id and lane masks (not volatile: the compiler may keep one read for
+// a whole loop instead of reading the special register at every use).
 __device__ __forceinline__ unsigned lane_id() {
   unsigned l;
-  asm volatile("mov.u32 %0, %%laneid;" : "=r"(l));
+  asm("mov.u32 %0, %%laneid;" : "=r"(l));
   return l;
 }
 __device__ __forceinline__ unsigned lanemask_lt() {
   unsigned m;
-  asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+  return m;
+}
+__device__ __forceinline__ unsigned lanemask_le() {
+  unsigned m;
+  asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));
   return m;
 }
 

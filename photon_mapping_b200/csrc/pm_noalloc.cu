@@ -116,9 +116,6 @@ extern "C" int pm_photonmap_radiance_noalloc(const float* d_photons,
   m.wi2 = wi2;
   m.boxes = boxes;
   m.n = (int)n_photons;
-  m.grid = nullptr;  // no cell grid: the searches walk the box tree
-  m.grid_lmax = 0;
-  for (int i = 0; i < kGridLevels; ++i) m.grid_off[i] = 0;
   map_build_launch(d_photons, (int)n_photons, pos4, thr4, wi2, boxes, lvl_off,
                    lvl_cnt, m.nlevels, sort, st);
   cudaError_t e = cudaGetLastError();

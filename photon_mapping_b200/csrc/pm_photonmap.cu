@@ -39,24 +39,6 @@ int map_levels(int64_t n, int* nlevels, int* lvl_off, int* lvl_cnt) {
   return off;
 }
 
-size_t grid_words(int64_t n, int* lmax, int* off) {
-  // finest level: about one cell per photon or coarser (8^L <= 8 n), at
-  // most kGridMaxLevel; maps too small for kGridMinLevel get no grid
-  int L = 0;
-  while (L < kGridMaxLevel && (int64_t)1 << (3 * (L + 1)) <= 8 * n) ++L;
-  if (n <= 0 || L < kGridMinLevel) {
-    *lmax = 0;
-    return 0;
-  }
-  *lmax = L;
-  size_t w = kGridHeader;
-  for (int l = kGridMinLevel; l <= L; ++l) {
-    off[l - kGridMinLevel] = (int)w;
-    w += ((size_t)1 << (3 * l)) + 1;
-  }
-  return w;
-}
-
 size_t map_build_scratch_bytes(int64_t n) {
   const size_t nn = (size_t)(n > 0 ? n : 1);
   // keys a/b, values a/b, tile histogram, bbox words
@@ -208,42 +190,10 @@ __global__ void node_box_kernel(float4* __restrict__ boxes, int child_off,
   }
 }
 
-// Finest grid level: the first sorted photon of each cell c (the first
-// key >= c << shift), for c in [0, ncells]; cell ncells gets n.
-__global__ void grid_finest_kernel(const uint32_t* __restrict__ keys, int n, int shift,
-                                   uint32_t ncells, uint32_t* __restrict__ tab) {
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c > ncells) return;
-  if (c == ncells) {
-    tab[c] = (uint32_t)n;
-    return;
-  }
-  const uint32_t want = c << shift;
-  int lo = 0, hi = n;  // lower bound in [lo, hi]
-  while (lo < hi) {
-    const int mid = (lo + hi) >> 1;
-    if (__ldg(keys + mid) < want) lo = mid + 1;
-    else hi = mid;
-  }
-  tab[c] = (uint32_t)lo;
-}
-
-// A coarser level: cell c starts where its first child cell 8c starts.
-__global__ void grid_coarser_kernel(const uint32_t* __restrict__ fine, uint32_t ncells,
-                                    uint32_t* __restrict__ tab) {
-  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c <= ncells) tab[c] = fine[(size_t)c << 3];
-}
-
-__global__ void grid_header_kernel(const uint32_t* __restrict__ bb, uint32_t* __restrict__ grid) {
-  if (threadIdx.x < 6) grid[threadIdx.x] = bb[threadIdx.x];
-  else if (threadIdx.x < kGridHeader) grid[threadIdx.x] = 0;
-}
-
 void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
                       float2* wi2, float4* boxes, const int* lvl_off,
                       const int* lvl_cnt, int nlevels, void* scratch,
-                      cudaStream_t st, uint32_t* grid, int grid_lmax, const int* grid_off) {
+                      cudaStream_t st) {
   if (n <= 0) return;
   uint32_t* ka = (uint32_t*)scratch;
   uint32_t* kb = ka + n;
@@ -265,20 +215,6 @@ void map_build_launch(const float* aos, int n, float4* pos4, float4* thr4,
   for (int l = 1; l < nlevels; ++l) {
     node_box_kernel<<<(lvl_cnt[l] * 32 + tb - 1) / tb, tb, 0, st>>>(
         boxes, lvl_off[l - 1], lvl_cnt[l - 1], lvl_off[l], lvl_cnt[l]);
-  }
-  if (grid && grid_lmax >= kGridMinLevel) {
-    grid_header_kernel<<<1, 32, 0, st>>>(bb, grid);
-    const uint32_t* keys = in_b ? kb : ka;
-    const int L = grid_lmax;
-    const uint32_t nc = 1u << (3 * L);
-    uint32_t* fine = grid + grid_off[L - kGridMinLevel];
-    grid_finest_kernel<<<(nc + 1 + tb - 1) / tb, tb, 0, st>>>(keys, n, 3 * (10 - L), nc, fine);
-    for (int l = L - 1; l >= kGridMinLevel; --l) {
-      const uint32_t ncl = 1u << (3 * l);
-      uint32_t* tab = grid + grid_off[l - kGridMinLevel];
-      grid_coarser_kernel<<<(ncl + 1 + tb - 1) / tb, tb, 0, st>>>(fine, ncl, tab);
-      fine = tab;
-    }
   }
 }
 
@@ -352,18 +288,11 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 struct Levels {
   int2 oc[kMaxLevels];  // {offset of the level's boxes, boxes in the level}
-  // the cell grid: finest level (0: not used), word offsets of the levels'
-  // tables, the box the Morton codes were made in, its smallest positive
-  // extent
-  int glmax;
-  int goff[kGridLevels];
-  float glo[3], gext[3];
-  float gmin_ext;
 };
 
 enum {
   kStatQueries = 0, kStatCold, kStatCand, kStatLeaves, kStatNodes, kStatSelects, kStatWalks,
-  kStatGrid, kNumStats
+  kNumStats
 };
 
 // Counters are compiled in only for the kernels launched with statistics.
@@ -689,16 +618,14 @@ __device__ __forceinline__ void scan_groups(const MapDev& m, Query& q,
   const int sub = lane >> 3, j = lane & 7;
   stat_add<S>(s, lane, kStatLeaves, (uint32_t)ng);
   for (int r = 0; r < ng; r += 8) {
+    // invalid lanes read group 0 / photon 0 and offer nothing (no divergent
+    // branch around the loads)
     const int ga = r + sub, gb = r + 4 + sub;
-    int ia = 0, ib = 0;
-    bool va = ga < ng, vb = gb < ng;
-    if (va) ia = (int)s.list[ga] * kGroup + j;
-    if (vb) ib = (int)s.list[gb] * kGroup + j;
-    va = va && ia < m.n;
-    vb = vb && ib < m.n;
-    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
-    if (va) pa = __ldg(m.pos4 + ia);
-    if (vb) pb = __ldg(m.pos4 + ib);
+    const int ia = (int)s.list[ga < ng ? ga : 0] * kGroup + j;
+    const int ib = (int)s.list[gb < ng ? gb : 0] * kGroup + j;
+    const bool va = ga < ng && ia < m.n, vb = gb < ng && ib < m.n;
+    const float4 pa = __ldg(m.pos4 + (va ? ia : 0));
+    const float4 pb = __ldg(m.pos4 + (vb ? ib : 0));
     offer<C, S>(m, q, s, lane, pa, ia, va);
     if (r + 4 < ng) offer<C, S>(m, q, s, lane, pb, ib, vb);
   }
@@ -713,9 +640,8 @@ __device__ __forceinline__ void scan_range(const MapDev& m, Query& q,
   for (int b = lo; b < hi; b += 64) {
     const int ia = b + lane, ib = b + 32 + lane;
     const bool va = ia < hi, vb = ib < hi;
-    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
-    if (va) pa = __ldg(m.pos4 + ia);
-    if (vb) pb = __ldg(m.pos4 + ib);
+    const float4 pa = __ldg(m.pos4 + (va ? ia : lo));
+    const float4 pb = __ldg(m.pos4 + (vb ? ib : lo));
     offer<C, S>(m, q, s, lane, pa, ia, va);
     if (b + 32 < hi) offer<C, S>(m, q, s, lane, pb, ib, vb);
   }
@@ -747,14 +673,14 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
     const int cl = (int)(e >> 28) - 1;  // level of the children
     const int c = (int)(e & 0x0fffffffu) * 32 + lane;
     stat_add<S>(s, lane, kStatNodes, 1);
-    bool pass = false;
+    // lanes past the level's end read its first box and do not pass (no
+    // divergent branch around the loads: 3 % of the kNN time)
     const int2 oc = L.oc[cl];
-    if (c < oc.y) {
-      const int jb = oc.x + c;
-      const float4 lo = __ldg(m.boxes + 2 * jb);
-      const float4 hi = __ldg(m.boxes + 2 * jb + 1);
-      pass = box_dist2(q.x, q.y, q.z, lo, hi) <= q.tau;
-    }
+    const bool in = c < oc.y;
+    const int jb = oc.x + (in ? c : 0);
+    const float4 lo = __ldg(m.boxes + 2 * jb);
+    const float4 hi = __ldg(m.boxes + 2 * jb + 1);
+    const bool pass = in && box_dist2(q.x, q.y, q.z, lo, hi) <= q.tau;
     const unsigned bal = __ballot_sync(kFull, pass);
     const int off = __popc(bal & lanemask_lt());
     if (cl == 0) {
@@ -781,180 +707,6 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
     }
     if (done) break;
   }
-}
-
-// Photons per bottom node of the box tree (32 groups of 8).
-constexpr int kNodeSpan = 32 * kGroup;
-
-__device__ __forceinline__ unsigned lanemask_le() {
-  unsigned m;
-  asm volatile("mov.u32 %0, %%lanemask_le;" : "=r"(m));
-  return m;
-}
-
-// Candidates from the cell grid: every photon with dist2 <= q.tau into the
-// warp buffer, in the order the tree walk meets them (bottom nodes of
-// kNodeSpan sorted photons in descending order, photons ascending within
-// one), so the kept photons, their order and their sum do not depend on
-// which of the two ran. Returns false, having appended nothing, when the
-// grid does not suit the radius r and the tree is walked instead:
-//   * the level is the finest whose cells are at least 2r/3 along every
-//     axis (so the query's box, 2r wide, meets at most 4 cells per axis,
-//     64 in all); it must not be coarser than kGridMinLevel;
-//   * the map's finest level must not be coarser than that by 2 levels or
-//     more (cells many times the sphere: the tree tests fewer photons);
-//   * the candidate cells must give at most 32 pieces (below).
-// The candidate cells are the build's own cells of q -+ r per axis (the
-// same cell function, with a margin for the rounding of q -+ r); a cell
-// whose box (widened by 1e-3 of a cell) is farther than sqrt(tau) is
-// skipped. A cell is one range of sorted photons, cut into pieces at
-// bottom-node boundaries; the pieces are ranked in the walk's order and
-// scanned as one stream, 32 photons per round.
-template <int C, bool S>
-__device__ __forceinline__ bool collect_grid(const MapDev& m, const Levels& L, Query& q,
-                                             WarpBuf<C>& s, int lane) {
-  const float r = sqrtf(q.tau);
-  if (!(r > 0.f) || !(r < __int_as_float(0x7f800000)) || !(fabsf(q.x) < 1e30f) ||
-      !(fabsf(q.y) < 1e30f) || !(fabsf(q.z) < 1e30f))
-    return false;
-  const float rr = r * 1.0001f;
-  const int lv = ilogbf(__fdividef(1.5f * L.gmin_ext, rr));
-  if (lv < kGridMinLevel || lv >= L.glmax + 2) return false;
-  const int lvl = min(lv, L.glmax);
-  const int sh = 10 - lvl;
-  int c0[3], nc[3];
-  const float qv[3] = {q.x, q.y, q.z};
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float mg = rr + fabsf(qv[a]) * 1e-6f;
-    c0[a] = (int)(cell10(qv[a] - mg, L.glo[a], L.gext[a]) >> sh);
-    nc[a] = (int)(cell10(qv[a] + mg, L.glo[a], L.gext[a]) >> sh) - c0[a] + 1;
-  }
-  if (nc[0] > 4 || nc[1] > 4 || nc[2] > 4) return false;
-  const float scale = __int_as_float((127 - lvl) << 23);  // 2^-lvl
-  const uint32_t* tab = m.grid + L.goff[lvl - kGridMinLevel];
-  // the candidate cells (slot t of 4 x 4 x 4 is (t & 3, t >> 2 & 3, t >> 4)),
-  // cut into pieces at bottom-node boundaries: s.stack[0..32) starts,
-  // s.stack[32..64) ends
-  int npc = 0;
-#pragma unroll
-  for (int h = 0; h < 2; ++h) {
-    const int t = lane + 32 * h;
-    const int dx = t & 3, dy = (t >> 2) & 3, dz = t >> 4;
-    bool use = dx < nc[0] && dy < nc[1] && dz < nc[2];
-    uint32_t b = 0, e = 0;
-    if (use) {
-      const int cx = c0[0] + dx, cy = c0[1] + dy, cz = c0[2] + dz;
-      const float sx = L.gext[0] * scale, sy = L.gext[1] * scale, sz = L.gext[2] * scale;
-      const float4 blo = make_float4(L.glo[0] + (float)cx * sx - sx * 1e-3f,
-                                     L.glo[1] + (float)cy * sy - sy * 1e-3f,
-                                     L.glo[2] + (float)cz * sz - sz * 1e-3f, 0.f);
-      const float4 bhi = make_float4(L.glo[0] + (float)(cx + 1) * sx + sx * 1e-3f,
-                                     L.glo[1] + (float)(cy + 1) * sy + sy * 1e-3f,
-                                     L.glo[2] + (float)(cz + 1) * sz + sz * 1e-3f, 0.f);
-      use = box_dist2(q.x, q.y, q.z, blo, bhi) <= q.tau;
-      if (use) {
-        const uint32_t code = (spread10((uint32_t)cx) << 2) | (spread10((uint32_t)cy) << 1) |
-                              spread10((uint32_t)cz);
-        b = __ldg(tab + code);
-        e = __ldg(tab + code + 1);
-        use = e > b;
-      }
-    }
-    const int cnt = use ? (int)(((e - 1) / kNodeSpan) - (b / kNodeSpan)) + 1 : 0;
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int y = __shfl_up_sync(kFull, incl, o);
-      if (lane >= o) incl += y;
-    }
-    const int tot = __shfl_sync(kFull, incl, 31);
-    if (npc + tot <= 32) {
-      int o = npc + incl - cnt;
-      for (uint32_t x = b; x < e; ++o) {
-        const uint32_t xe = min(e, (x / kNodeSpan + 1) * kNodeSpan);
-        s.stack[o] = x;
-        s.stack[32 + o] = xe;
-        x = xe;
-      }
-    }
-    npc += tot;
-  }
-  if (npc > 32) return false;
-  __syncwarp();
-  // rank the pieces in the walk's order, then piece j in lane j
-  uint32_t pb = 0, pe = 0, key = 0xffffffffu;
-  if (lane < npc) {
-    pb = s.stack[lane];
-    pe = s.stack[32 + lane];
-    key = ((0x7fffffu - pb / kNodeSpan) << 8) | (pb % kNodeSpan);
-  }
-  int rank = 0;
-  for (int t = 0; t < npc; ++t) rank += __shfl_sync(kFull, key, t) < key;
-  if (lane < npc) {
-    s.stack[64 + rank] = pb;
-    s.stack[96 + rank] = pe;
-  }
-  __syncwarp();
-  uint32_t sb = 0, len = 0;
-  if (lane < npc) {
-    sb = s.stack[64 + lane];
-    len = s.stack[96 + lane] - sb;
-  }
-  uint32_t incl = len;
-#pragma unroll
-  for (int o = 1; o < 32; o <<= 1) {
-    const uint32_t y = __shfl_up_sync(kFull, incl, o);
-    if (lane >= o) incl += y;
-  }
-  const uint32_t total = __shfl_sync(kFull, incl, 31);
-  const uint32_t off = incl - len;  // stream offset of piece `lane`
-  q.cnt = 0;
-  stat_add<S>(s, lane, kStatWalks, 1);
-  stat_add<S>(s, lane, kStatGrid, 1);
-  stat_add<S>(s, lane, kStatLeaves, (uint32_t)npc);
-  // the stream, two rounds of 32 loaded before either is offered; the
-  // piece of stream index t is the last piece starting at or before t
-  int before = 0;
-  for (uint32_t r0 = 0; r0 < total; r0 += 64) {
-    int ia = 0, ib = 0;
-    bool va, vb;
-    {
-      const uint32_t bit = lane < npc && off >= r0 && off < r0 + 32 ? 1u << (off - r0) : 0u;
-      const uint32_t starts = __reduce_or_sync(kFull, bit);
-      const int j = before + __popc(starts & lanemask_le()) - 1;
-      before += __popc(starts);
-      const uint32_t t = r0 + lane;
-      va = t < total;
-      ia = (int)(__shfl_sync(kFull, sb, j & 31) + (t - __shfl_sync(kFull, off, j & 31)));
-    }
-    {
-      const uint32_t r1 = r0 + 32;
-      const uint32_t bit = lane < npc && off >= r1 && off < r1 + 32 ? 1u << (off - r1) : 0u;
-      const uint32_t starts = __reduce_or_sync(kFull, bit);
-      const int j = before + __popc(starts & lanemask_le()) - 1;
-      before += __popc(starts);
-      const uint32_t t = r1 + lane;
-      vb = t < total;
-      ib = (int)(__shfl_sync(kFull, sb, j & 31) + (t - __shfl_sync(kFull, off, j & 31)));
-    }
-    float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pbv = pa;
-    if (va) pa = __ldg(m.pos4 + ia);
-    if (vb) pbv = __ldg(m.pos4 + ib);
-    offer<C, S>(m, q, s, lane, pa, ia, va);
-    if (r0 + 32 < total) offer<C, S>(m, q, s, lane, pbv, ib, vb);
-  }
-  __syncwarp();
-  return true;
-}
-
-// Candidates of query q: from the cell grid when it suits, else by the
-// tree walk.
-template <int C, bool S>
-__device__ __forceinline__ void gather(const MapDev& m, const Levels& L, Query& q,
-                                       WarpBuf<C>& s, int lane) {
-  if (L.glmax > 0 && collect_grid<C, S>(m, L, q, s, lane)) return;
-  collect<C, S>(m, L, q, s, lane);
 }
 
 __device__ __forceinline__ unsigned long long warp_min_u64(
@@ -1117,7 +869,7 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
           need_cold = false;
           guess = false;
         }
-        gather<C, S>(m, L, q, s, lane);
+        collect<C, S>(m, L, q, s, lane);
         if (warm_guess) {
           if (q.cnt >= k) break;
           warm_guess = false;
@@ -1276,40 +1028,22 @@ __device__ __forceinline__ void knn_chunk(const MapDev& m, const Levels& L, Warp
   }
 }
 
-// The tree shape and the cell grid's description of map m (one thread):
-// the grid is used when `grid` is set and the map has one.
-__device__ __forceinline__ void load_levels(const MapDev& m, Levels& L, bool grid) {
-#pragma unroll
-  for (int i = 0; i < kMaxLevels; ++i)  // constant indices: m stays in
-    L.oc[i] = make_int2(m.lvl_off[i], m.lvl_cnt[i]);  // the parameter bank
-  L.glmax = grid && m.grid ? m.grid_lmax : 0;
-#pragma unroll
-  for (int i = 0; i < kGridLevels; ++i) L.goff[i] = m.grid_off[i];
-  float mn = __int_as_float(0x7f800000);
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    // the box as the build's morton_kernel reads it
-    const float lo = L.glmax ? from_ordered(m.grid[a]) : 0.f;
-    const float ext = L.glmax ? from_ordered(m.grid[3 + a]) - lo : 0.f;
-    L.glo[a] = lo;
-    L.gext[a] = ext;
-    if (ext > 0.f) mn = fminf(mn, ext);
-  }
-  L.gmin_ext = mn < __int_as_float(0x7f800000) ? mn : 0.f;
-}
-
 template <int C, int MODE, bool S>
 __global__ void __launch_bounds__(256, 4)
     knn_kernel(MapDev m, const void* __restrict__ queries, int64_t nq, int k,
                float n_emitted, KnnOut out,
                unsigned long long* __restrict__ counter,
-               const uint32_t* __restrict__ order, int stride4, int64_t head_items,
-               int grid) {
+               const uint32_t* __restrict__ order, int stride4, int64_t head_items) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ Levels L;
   WarpBuf<C>& s = reinterpret_cast<WarpBuf<C>*>(smem_raw)[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  if (threadIdx.x == 0) load_levels(m, L, grid != 0);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int i = 0; i < kMaxLevels; ++i) {  // constant indices: m stays in
+      L.oc[i] = make_int2(m.lvl_off[i], m.lvl_cnt[i]);  // the parameter bank
+    }
+  }
   if (lane < 8) s.stat[lane] = 0;
   __syncthreads();
   float r_hint = -1.f;  // last exact k-th distance this warp found
@@ -1342,7 +1076,7 @@ static cudaError_t launch_one(const MapDev& m, const void* queries,
                               int64_t nq, int k, float n_emitted, KnnOut out,
                               unsigned long long* counter, int num_sms,
                               cudaStream_t st, const uint32_t* order,
-                              int stride4, bool grid) {
+                              int stride4) {
   constexpr int kThreads = (C <= 512) ? 256 : 128;
   const size_t smem = (kThreads / 32) * sizeof(WarpBuf<C>);
   auto kern = out.stats ? knn_kernel<C, MODE, true> : knn_kernel<C, MODE, false>;
@@ -1365,36 +1099,33 @@ static cudaError_t launch_one(const MapDev& m, const void* queries,
   e = cudaMemsetAsync(counter, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
   kern<<<(unsigned)blocks, kThreads, smem, st>>>(m, queries, nq, k, n_emitted,
-                                                 out, counter, order, stride4, head_items,
-                                                 grid ? 1 : 0);
+                                                 out, counter, order, stride4, head_items);
   return cudaGetLastError();
-}
-
-template <int MODE>
-static cudaError_t launch_mode(const MapDev& m, const void* queries, int64_t nq, int k,
-                               float n_emitted, KnnOut out, unsigned long long* counter,
-                               int num_sms, cudaStream_t st, const uint32_t* order, int stride4,
-                               bool grid) {
-  if (k <= 224)
-    return launch_one<512, MODE>(m, queries, nq, k, n_emitted, out, counter, num_sms, st, order,
-                                 stride4, grid);
-  return launch_one<2048, MODE>(m, queries, nq, k, n_emitted, out, counter, num_sms, st, order,
-                                stride4, grid);
 }
 
 cudaError_t knn_launch(const MapDev& m, const void* queries, int64_t nq,
                        int k, int mode, float n_emitted, KnnOut out,
                        unsigned long long* counter, int num_sms,
-                       cudaStream_t st, const uint32_t* order, int stride4, bool grid) {
+                       cudaStream_t st, const uint32_t* order, int stride4) {
   if (nq <= 0) return cudaSuccess;
-  if (mode == kModeAdjoint)
-    return launch_mode<kModeAdjoint>(m, queries, nq, k, n_emitted, out, counter, num_sms, st,
-                                     order, stride4, grid);
-  if (mode == kModeRadiance)
-    return launch_mode<kModeRadiance>(m, queries, nq, k, n_emitted, out, counter, num_sms, st,
-                                      order, stride4, grid);
-  return launch_mode<kModeKnn>(m, queries, nq, k, n_emitted, out, counter, num_sms, st, order,
-                               stride4, grid);
+  if (mode == kModeAdjoint) {
+    return k <= 224 ? launch_one<512, kModeAdjoint>(m, queries, nq, k, n_emitted, out, counter,
+                                                   num_sms, st, order, stride4)
+                    : launch_one<2048, kModeAdjoint>(m, queries, nq, k, n_emitted, out, counter,
+                                                    num_sms, st, order, stride4);
+  }
+  if (k <= 224) {
+    return mode == kModeRadiance
+               ? launch_one<512, kModeRadiance>(m, queries, nq, k, n_emitted,
+                                                out, counter, num_sms, st, order, stride4)
+               : launch_one<512, kModeKnn>(m, queries, nq, k, n_emitted, out,
+                                           counter, num_sms, st, order, stride4);
+  }
+  return mode == kModeRadiance
+             ? launch_one<2048, kModeRadiance>(m, queries, nq, k, n_emitted,
+                                               out, counter, num_sms, st, order, stride4)
+             : launch_one<2048, kModeKnn>(m, queries, nq, k, n_emitted, out,
+                                          counter, num_sms, st, order, stride4);
 }
 
 }  // namespace pm
@@ -1436,7 +1167,9 @@ __global__ void __launch_bounds__(256, 4)
       if (lane == 0) {
         const BatchScene& bs = t.scenes[sc];
         wmap[warp] = bs.map;
-        load_levels(bs.map, wlev[warp], true);
+        for (int i = 0; i < kMaxLevels; ++i) {
+          wlev[warp].oc[i] = make_int2(bs.map.lvl_off[i], bs.map.lvl_cnt[i]);
+        }
       }
       __syncwarp();
       cur = sc;

@@ -72,15 +72,13 @@ def test_struct_layouts_match_the_header(tmp_path):
     src = tmp_path / "sizes.c"
     src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "pm_cuda.h"\n'
                    'int main(void) {\n'
-                   '  printf("%zu %zu %zu %zu %zu %zu\\n", sizeof(pm_trace_stats),\n'
+                   '  printf("%zu %zu %zu %zu %zu\\n", sizeof(pm_trace_stats),\n'
                    '         offsetof(pm_trace_stats, rays), sizeof(pm_render_stats),\n'
-                   '         offsetof(pm_render_stats, rays), sizeof(pm_knn_stats),\n'
-                   '         offsetof(pm_knn_stats, grid_searches));\n'
+                   '         offsetof(pm_render_stats, rays), sizeof(pm_knn_stats));\n'
                    '  return 0;\n}\n')
     exe = tmp_path / "sizes"
     subprocess.run(["gcc", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
     got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
                                           check=True).stdout.split()]
     assert got == [C.sizeof(TraceStats), TraceStats.rays.offset, C.sizeof(RenderStats),
-                   RenderStats.rays.offset, 8 * len(N.Context.STAT_FIELDS),
-                   8 * N.Context.STAT_FIELDS.index("grid_searches")]
+                   RenderStats.rays.offset, 8 * len(N.Context.STAT_FIELDS)]

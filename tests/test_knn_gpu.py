@@ -284,68 +284,3 @@ def test_stats_counters(ctx):
     assert st["selects"] >= 1
     pm.radiance(q, 50, 50000)
     assert all(v == 0 for v in ctx.get_stats().values())
-
-
-@pytest.mark.parametrize("k", [1, 16, 50, 100, 256])
-def test_grid_changes_nothing(ctx, k):
-    """Cell-grid searches (pm_ctx_set_knn_grid) answer most queries of a
-    coherent stream, and give the same lists, distances and radiance, bit
-    for bit, as tree walks alone; both equal brute force."""
-    ph = W.wall_photons(120000, 300 + k)
-    q = W.wall_queries(6000, 400 + k)
-    q = q[np.lexsort((q[:, 2], q[:, 1], q[:, 0]))]  # spatially coherent order
-    pm = gpu_map(ctx, ph)
-    results = {}
-    for grid in (True, False):
-        ctx.set_knn_grid(grid)
-        ctx.get_stats(reset=True)
-        ctx.set_stats(True)
-        try:
-            lists = pm.query_knn(q[:, :3], k)
-            rad = pm.radiance(q, k, 120000)
-            st = ctx.get_stats(reset=True)
-        finally:
-            ctx.set_stats(False)
-            ctx.set_knn_grid(True)
-        results[grid] = (lists, rad, st)
-    (a, ra, sa), (b, rb, sb) = results[True], results[False]
-    for x, y in zip(a, b):
-        np.testing.assert_array_equal(x, y)
-    np.testing.assert_array_equal(ra, rb)
-    assert sb["grid_searches"] == 0
-    # k = 1: radii far below the finest cells, the tree serves them
-    assert sa["grid_searches"] > (0.5 if k >= 16 else 0.0) * sa["walks"], sa
-    sample = np.arange(0, q.shape[0], 7)
-    oidx, ocnt, omd2 = O.knn(ph, q[sample, :3], k)
-    np.testing.assert_array_equal(a[0][sample], oidx)
-    np.testing.assert_array_equal(a[2][sample], omd2)
-    assert_radiance_close(ra[sample], O.radiance_fp64(ph, oidx, ocnt, omd2, q[sample], 120000),
-                          what=f"k={k}")
-
-
-def test_grid_with_ties_duplicates_and_flat_sets(ctx):
-    """Photons on a lattice (many equal distances), repeated photons and a
-    photon set with no extent along one axis: grid searches equal tree walks
-    and brute force."""
-    lat = W.lattice_photons(12, 0.125, seed=4)
-    dup = np.repeat(W.wall_photons(3000, 5), 3, axis=0)
-    flat = W.wall_photons(20000, 6)
-    flat[:, 4] = np.float32(0.25)         # every photon on the plane y = 0.25
-    for ph in (lat, dup, flat):
-        pm = gpu_map(ctx, ph)
-        rng = np.random.default_rng(6)
-        q = ph[rng.choice(ph.shape[0], 2000), 3:6].copy()
-        q[1::2] += rng.normal(scale=0.01, size=q[1::2].shape).astype(np.float32)
-        q = q[np.lexsort((q[:, 2], q[:, 1], q[:, 0]))]
-        got = {}
-        for grid in (True, False):
-            ctx.set_knn_grid(grid)
-            try:
-                got[grid] = pm.query_knn(q, 40)
-            finally:
-                ctx.set_knn_grid(True)
-        for x, y in zip(got[True], got[False]):
-            np.testing.assert_array_equal(x, y)
-        want = O.knn(ph, q, 40)
-        for x, y in zip(got[True], want):
-            np.testing.assert_array_equal(x, y)
