@@ -63,6 +63,11 @@ def parse_args():
                     help="instead of the benchmark: image error against the path tracer for "
                          "these configs (default 1 2 3), beside the reference integrator's")
     ap.add_argument("--pt-spp", type=int, default=4096)
+    ap.add_argument("--trace-render", choices=["cornell", "caustics"], default=None,
+                    help="instead of the benchmark: trace the photon maps of this scene twice "
+                         "(1M global photons, caustics x10 with the caustics scene) and render "
+                         "one 256x256 frame at 2 spp with final gathering; prints the rays and "
+                         "kernel times (a short run for profiling the trace and camera kernels)")
     return ap.parse_args()
 
 
@@ -380,13 +385,23 @@ def render_rates(ctx, sc, mesh, camera, dev, cpu: bool) -> dict:
         out[name] = {"samples_per_s": n / dt, "seconds": dt, "repeats": RENDER_REPEATS, **c,
                      "queries_global": st["queries_global"],
                      "queries_caustics": st["queries_caustics"], "passes": st["passes"],
-                     "mean_radiance": float(img.mean())}
+                     "mean_radiance": float(img.mean()),
+                     # closest-hit queries of the camera pass (camera, specular,
+                     # shadow and gather rays) over its kernels' device time
+                     "camera_rays": st["rays"], "camera_ms": st["camera_ms"],
+                     "camera_rays_per_s": st["rays"] / (st["camera_ms"] / 1e3)
+                     if st["camera_ms"] > 0 else None,
+                     "estimate_ms": st["estimate_ms"]}
         if trace_s is not None:
+            rays = sum(int(v["rays"]) for v in trace.values())
+            kms = sum(float(v["trace_ms"]) for v in trace.values())
             out[name]["photon_trace"] = {
                 "seconds": trace_s, "triangles": int(scene_mesh.n_faces),
                 "emitted": c["photons"] + int(c["photons"] * mult),
                 "stored": {k: int(v["stored"]) for k, v in trace.items()},
-                "photons_per_s": (c["photons"] + c["photons"] * mult) / trace_s}
+                "photons_per_s": (c["photons"] + c["photons"] * mult) / trace_s,
+                "rays": rays, "trace_kernel_ms": kms,
+                "rays_per_s": rays / (kms / 1e3) if kms > 0 else None}
         if cpu and c.get("scene") != "caustics":
             out[name]["cpu_reference"] = cpu_render_rate(mesh, pmi, c)
         if scene_dev is not sc:
@@ -491,7 +506,7 @@ def batched_rates(n_scenes: int, dev) -> dict:
     torch.cuda.synchronize(dev)
     br = B.BatchRenderer(scenes)
     t0 = time.perf_counter()
-    best, stage_ms = br.autotune()
+    best, tune_ms = br.autotune()
     tune_s = time.perf_counter() - t0
     br.render(use_graph=True)                      # capture + warm-up
     br.render(use_graph=True)
@@ -501,6 +516,8 @@ def batched_rates(n_scenes: int, dev) -> dict:
         dev_ms.append(br.render(use_graph=True))
         wall_s.append(time.perf_counter() - t0)
     nograph_ms = br.render(use_graph=False)
+    stage_ms = [br.stage_times() for _ in range(3)]
+    stages = {k: min(st[k] for st in stage_ms) for k in stage_ms[0]}
     max_diff = max(float(np.abs(br.image(i) - imgs[i]).max()) for i in range(n_scenes))
     stored, queries = br.counts()
     br.close()
@@ -526,7 +543,8 @@ def batched_rates(n_scenes: int, dev) -> dict:
         "batched_vs_sequential": seq_step / step_s,
         "max_abs_image_difference": max_diff,
         "tuning": best,
-        "tuned_stage_ms": {"trace": stage_ms[0], "camera": stage_ms[1], "knn": stage_ms[2]},
+        "autotune_stage_ms": {"trace": tune_ms[0], "camera": tune_ms[1], "knn": tune_ms[2]},
+        "stage_ms": stages,
         "autotune_s": tune_s,
     }
 
@@ -684,7 +702,12 @@ def run_ours(args) -> None:
         "knn_uniform_cube": uniform,
         "photon_trace": {"emitted": N_EMIT, "stored": trace_stats["stored"],
                          "seconds": trace_s, "photons_per_s": N_EMIT / trace_s,
-                         "includes": "emission, tracing, ordering and the map build"},
+                         "includes": "emission, tracing, ordering and the map build",
+                         "rays": trace_stats["rays"],
+                         "trace_kernel_ms": trace_stats["trace_ms"],
+                         "build_ms": trace_stats["build_ms"],
+                         "rays_per_s": trace_stats["rays"] / (trace_stats["trace_ms"] / 1e3)
+                         if trace_stats["trace_ms"] > 0 else None},
         "render": render,
         "gradient": grad,
         "batched": batched,
@@ -805,9 +828,33 @@ def run_reference(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def run_trace_render(args) -> None:
+    from photon_mapping_b200 import Context
+    from photon_mapping_b200 import scene as S
+    from photon_mapping_b200.integrator import PhotonMapping
+    caustics = args.trace_render == "caustics"
+    mesh = S.caustics_scene(0) if caustics else S.cornell_box(0)
+    _, camera = scene_and_camera()
+    ctx = Context(0)
+    sc = S.Scene(ctx)
+    sc.setMesh(mesh)
+    sc.build()
+    pmi = PhotonMapping(N_EMIT, K_NEAREST, 10.0 if caustics else 1.0, K_NEAREST, 1, MAX_DEPTH,
+                        ctx=ctx)
+    pmi.build(sc, seed=TRACE_SEED)
+    trace = pmi.build(sc, seed=TRACE_SEED)
+    img, st = pmi.render(camera, 256, 256, 2)
+    print(json.dumps({"scene": args.trace_render, "triangles": int(mesh.n_faces),
+                      "trace": trace, "render": st, "mean_radiance": float(img.mean())}),
+          flush=True)
+    ctx.close()
+
+
 def main():
     args = parse_args()
-    if args.convergence is not None:
+    if args.trace_render is not None:
+        run_trace_render(args)
+    elif args.convergence is not None:
         run_convergence(args)
     elif args.impl == "reference":
         run_reference(args)

@@ -459,6 +459,19 @@ int pm_batch_counts(pm_batch* batch, int64_t* photons_stored, int64_t* queries);
  * scene (integrator.h:406-469; the counterpart of pm_photonmap_get_photons). */
 int pm_batch_photons(pm_batch* batch, int32_t scene, float* out_photons);
 
+/* Stages of one batched step, in order, for pm_batch_stage_times. */
+#define PM_BATCH_STAGE_TRACE 0   /* photon emission and tracing, every scene   */
+#define PM_BATCH_STAGE_MAPS 1    /* photon order and map build, every scene    */
+#define PM_BATCH_STAGE_CAMERA 2  /* camera pass and the listing of the queries */
+#define PM_BATCH_STAGE_SORT 3    /* sort of the queries by (scene, Morton)     */
+#define PM_BATCH_STAGE_KNN 4     /* query ranges and the radiance estimates    */
+#define PM_BATCH_STAGE_RESOLVE 5 /* samples into the images                    */
+#define PM_BATCH_STAGES 6
+/* Runs one step without a graph, timing each stage with CUDA events, and
+ * writes min(n, PM_BATCH_STAGES) times in ms. The step's results are those
+ * of pm_batch_render. */
+int pm_batch_stage_times(pm_batch* batch, float* ms, int32_t n);
+
 #ifdef __cplusplus
 }
 #endif

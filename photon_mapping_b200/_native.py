@@ -81,6 +81,7 @@ _SIGNATURES = {
     "pm_batch_image": (C.c_int, [_vp, C.c_int32, _vp]),
     "pm_batch_counts": (C.c_int, [_vp, _vp, _vp]),
     "pm_batch_photons": (C.c_int, [_vp, C.c_int32, _vp]),
+    "pm_batch_stage_times": (C.c_int, [_vp, _vp, C.c_int32]),
 }
 
 

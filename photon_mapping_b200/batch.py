@@ -144,6 +144,15 @@ class BatchRenderer:
                                             C.addressof(ms)), "pm_batch_render")
         return float(ms.value)
 
+    STAGES = ("trace", "maps", "camera", "sort", "knn", "resolve")
+
+    def stage_times(self) -> dict:
+        """One step without a graph, each stage timed on the device (ms)."""
+        ms = (C.c_float * len(self.STAGES))()
+        self.check(self.lib.pm_batch_stage_times(self.handle, C.addressof(ms), len(ms)),
+                   "pm_batch_stage_times")
+        return {k: float(v) for k, v in zip(self.STAGES, ms)}
+
     def image(self, i: int) -> np.ndarray:
         sc = self.scenes[i]
         out = np.empty((sc["height"], sc["width"], 3), np.float32)

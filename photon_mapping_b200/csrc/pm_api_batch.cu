@@ -662,6 +662,47 @@ int pm_batch_autotune(pm_batch* b, pm_batch_tuning* best, float* ms_stage) {
   return check_step(b, "autotune");
 }
 
+int pm_batch_stage_times(pm_batch* b, float* ms, int32_t n) {
+  if (!b || !ms || n < 1) return PM_ERR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lk(b->mu);
+  cudaSetDevice(b->device);
+  cudaEvent_t ev[PM_BATCH_STAGES + 1] = {};
+  struct Guard {
+    cudaEvent_t* e;
+    ~Guard() {
+      for (int i = 0; i <= PM_BATCH_STAGES; ++i)
+        if (e[i]) cudaEventDestroy(e[i]);
+    }
+  } guard{ev};
+  cudaError_t e;
+  for (int i = 0; i <= PM_BATCH_STAGES; ++i)
+    if ((e = cudaEventCreate(&ev[i]))) return bcuda(b, e, "stage events");
+  const pm_batch_tuning& t = b->tune;
+  cudaMemsetAsync(b->err_word.ptr, 0, 4, b->st);
+  cudaEventRecord(ev[0], b->st);
+  enqueue_trace(b, t.block, t.bvh_stack);
+  cudaEventRecord(ev[1], b->st);
+  enqueue_maps(b);
+  cudaEventRecord(ev[2], b->st);
+  enqueue_camera_and_list(b, t.block, t.bvh_stack);
+  cudaEventRecord(ev[3], b->st);
+  const uint32_t* order = enqueue_sort(b);
+  cudaEventRecord(ev[4], b->st);
+  if ((e = enqueue_knn(b, order, t, b->knn_per_sm))) return bcuda(b, e, "stage times");
+  cudaEventRecord(ev[5], b->st);
+  batch_resolve_launch(b->tables, b->total_pix, b->st);
+  cudaEventRecord(ev[6], b->st);
+  if ((e = cudaGetLastError())) return bcuda(b, e, "stage times");
+  int s;
+  if ((s = check_step(b, "stage times")) != PM_OK) return s;
+  for (int i = 0; i < std::min<int>(n, PM_BATCH_STAGES); ++i) {
+    float x = 0.f;
+    cudaEventElapsedTime(&x, ev[i], ev[i + 1]);
+    ms[i] = x;
+  }
+  return PM_OK;
+}
+
 int pm_batch_image(pm_batch* b, int32_t scene, float* out) {
   if (!b) return PM_ERR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lk(b->mu);

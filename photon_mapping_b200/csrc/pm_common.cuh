@@ -71,4 +71,34 @@ __device__ __forceinline__ float box_dist2(float qx, float qy, float qz,
                    __fmul_rn(dz, dz));
 }
 
+// Low 10 bits of x spread to every third bit (one axis of a 30-bit Morton
+// code).
+__device__ __forceinline__ uint32_t spread10(uint32_t x) {
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+// Cell (0..1023) of coordinate v along an axis of the box [lo, lo + ext]
+// (NaN and values below lo: cell 0).
+__device__ __forceinline__ uint32_t cell10(float v, float lo, float ext) {
+  if (!(ext > 0.f)) return 0;
+  const float t = (v - lo) / ext * 1024.f;
+  if (!(t > 0.f)) return 0;
+  return t >= 1023.f ? 1023u : (uint32_t)t;
+}
+
+// Float <-> unsigned with the same order (negative floats reversed), for
+// atomicMin / atomicMax on floats.
+__device__ __forceinline__ uint32_t ordered_bits(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float from_ordered(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
 }  // namespace pm

@@ -45,13 +45,6 @@ size_t map_build_scratch_bytes(int64_t n) {
   return 4 * nn * sizeof(uint32_t) + sort_hist_words(nn) * 4 + 64;
 }
 
-__device__ __forceinline__ uint32_t ordered_bits(float f) {
-  const uint32_t u = __float_as_uint(f);
-  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float from_ordered(uint32_t u) {
-  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
 
 __global__ void bbox_kernel(const float* __restrict__ aos, int n,
                             uint32_t* __restrict__ bb) {
@@ -81,22 +74,6 @@ __global__ void bbox_kernel(const float* __restrict__ aos, int n,
       atomicMax(&bb[3 + a], ordered_bits(hi[a]));
     }
   }
-}
-
-__device__ __forceinline__ uint32_t spread10(uint32_t x) {
-  x &= 0x3ffu;
-  x = (x | (x << 16)) & 0x030000ffu;
-  x = (x | (x << 8)) & 0x0300f00fu;
-  x = (x | (x << 4)) & 0x030c30c3u;
-  x = (x | (x << 2)) & 0x09249249u;
-  return x;
-}
-
-__device__ __forceinline__ uint32_t cell10(float v, float lo, float ext) {
-  if (!(ext > 0.f)) return 0;
-  float t = (v - lo) / ext * 1024.f;
-  if (!(t > 0.f)) return 0;  // also NaN
-  return t >= 1023.f ? 1023u : (uint32_t)t;
 }
 
 __global__ void morton_kernel(const float* __restrict__ aos, int n,

@@ -229,15 +229,6 @@ __global__ void rng_init_kernel(unsigned long long* st, int w, int n) {
   st[p] = (unsigned long long)(j + w * i);  // UniformSampler(j + width * i)
 }
 
-__device__ __forceinline__ uint32_t spread10r(uint32_t x) {
-  x &= 0x3ffu;
-  x = (x | (x << 16)) & 0x030000ffu;
-  x = (x | (x << 8)) & 0x0300f00fu;
-  x = (x | (x << 4)) & 0x030c30c3u;
-  x = (x | (x << 2)) & 0x09249249u;
-  return x;
-}
-
 // Lists the slots holding a query of `map`, with the Morton code of the
 // query position (in the scene box) as the sort key.
 __global__ void list_queries_kernel(const float4* __restrict__ slots,
@@ -272,9 +263,9 @@ __global__ void list_queries_kernel(const float4* __restrict__ slots,
     if (!(c > 0.f)) return 0u;
     return c >= 1023.f ? 1023u : (uint32_t)c;
   };
-  keys[o] = (spread10r(cell(r0.x, lo.x, inv_ext.x)) << 2) |
-            (spread10r(cell(r0.y, lo.y, inv_ext.y)) << 1) |
-            spread10r(cell(r0.z, lo.z, inv_ext.z));
+  keys[o] = (spread10(cell(r0.x, lo.x, inv_ext.x)) << 2) |
+            (spread10(cell(r0.y, lo.y, inv_ext.y)) << 1) |
+            spread10(cell(r0.z, lo.z, inv_ext.z));
   vals[o] = (uint32_t)t;
 }
 
@@ -557,9 +548,9 @@ __global__ void __launch_bounds__(256)
     if (!(c > 0.f)) return 0u;
     return c >= 1023.f ? 1023u : (uint32_t)c;
   };
-  const uint32_t mc = (spread10r(cell(r0.x, bs.qlo.x, bs.qinv.x)) << 2) |
-                      (spread10r(cell(r0.y, bs.qlo.y, bs.qinv.y)) << 1) |
-                      spread10r(cell(r0.z, bs.qlo.z, bs.qinv.z));
+  const uint32_t mc = (spread10(cell(r0.x, bs.qlo.x, bs.qinv.x)) << 2) |
+                      (spread10(cell(r0.y, bs.qlo.y, bs.qinv.y)) << 1) |
+                      spread10(cell(r0.z, bs.qlo.z, bs.qinv.z));
   keys[o] = ((unsigned long long)s << 30) | mc;
   vals[o] = (uint32_t)g;
 }

@@ -34,14 +34,6 @@ __global__ void face_setup_kernel(const float* __restrict__ verts,
   geo[f] = make_float4(g.x, g.y, g.z, 0.5f * length(c));
 }
 
-__device__ __forceinline__ uint32_t ordered_f(float f) {
-  const uint32_t u = __float_as_uint(f);
-  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float unordered_f(uint32_t u) {
-  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
-
 __global__ void scene_bbox_kernel(const float4* __restrict__ tri, int n,
                                   uint32_t* __restrict__ bb) {
   float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX};
@@ -62,26 +54,10 @@ __global__ void scene_bbox_kernel(const float4* __restrict__ tri, int n,
   }
   if ((threadIdx.x & 31) == 0) {
     for (int a = 0; a < 3; ++a) {
-      atomicMin(&bb[a], ordered_f(lo[a]));
-      atomicMax(&bb[3 + a], ordered_f(hi[a]));
+      atomicMin(&bb[a], ordered_bits(lo[a]));
+      atomicMax(&bb[3 + a], ordered_bits(hi[a]));
     }
   }
-}
-
-__device__ __forceinline__ uint32_t spread10b(uint32_t x) {
-  x &= 0x3ffu;
-  x = (x | (x << 16)) & 0x030000ffu;
-  x = (x | (x << 8)) & 0x0300f00fu;
-  x = (x | (x << 4)) & 0x030c30c3u;
-  x = (x | (x << 2)) & 0x09249249u;
-  return x;
-}
-
-__device__ __forceinline__ uint32_t cell10b(float v, float lo, float ext) {
-  if (!(ext > 0.f)) return 0;
-  const float t = (v - lo) / ext * 1024.f;
-  if (!(t > 0.f)) return 0;
-  return t >= 1023.f ? 1023u : (uint32_t)t;
 }
 
 __global__ void tri_morton_kernel(const float4* __restrict__ tri, int n,
@@ -92,16 +68,16 @@ __global__ void tri_morton_kernel(const float4* __restrict__ tri, int n,
   if (f >= n) return;
   float lo[3], ext[3];
   for (int a = 0; a < 3; ++a) {
-    lo[a] = unordered_f(bb[a]);
-    ext[a] = unordered_f(bb[3 + a]) - lo[a];
+    lo[a] = from_ordered(bb[a]);
+    ext[a] = from_ordered(bb[3 + a]) - lo[a];
   }
   const float4 a = tri[3 * f], b = tri[3 * f + 1], c = tri[3 * f + 2];
   const float cx = (a.x + b.x + c.x) * (1.0f / 3.0f);
   const float cy = (a.y + b.y + c.y) * (1.0f / 3.0f);
   const float cz = (a.z + b.z + c.z) * (1.0f / 3.0f);
-  keys[f] = (spread10b(cell10b(cx, lo[0], ext[0])) << 2) |
-            (spread10b(cell10b(cy, lo[1], ext[1])) << 1) |
-            spread10b(cell10b(cz, lo[2], ext[2]));
+  keys[f] = (spread10(cell10(cx, lo[0], ext[0])) << 2) |
+            (spread10(cell10(cy, lo[1], ext[1])) << 1) |
+            spread10(cell10(cz, lo[2], ext[2]));
   vals[f] = (uint32_t)f;
 }
 
@@ -175,7 +151,7 @@ __global__ void refit_kernel(const float4* __restrict__ mt, int n,
   // padding: 4e-5 of the scene's size (largest extent or coordinate)
   float size = 0.f;
   for (int a = 0; a < 3; ++a) {
-    const float lo = unordered_f(bb[a]), hi = unordered_f(bb[3 + a]);
+    const float lo = from_ordered(bb[a]), hi = from_ordered(bb[3 + a]);
     size = fmaxf(size, fmaxf(hi - lo, fmaxf(fabsf(lo), fabsf(hi))));
   }
   const float pad = 4e-5f * size + 1e-30f;
