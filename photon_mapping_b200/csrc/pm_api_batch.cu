@@ -26,23 +26,14 @@ using namespace pm;
 
 static_assert(PM_BATCH_MAX_SCENES == kMaxBatchScenes, "batch limit");
 
-namespace {
-
-constexpr int kSideStreams = 8;
-
-}  // namespace
-
 struct pm_batch {
   std::mutex mu;  // calls on one batch are serialised
   int device = 0, num_sms = 148;
   cudaStream_t st = nullptr;
-  cudaStream_t side[kSideStreams] = {};
-  cudaEvent_t ev_fork = nullptr, ev0 = nullptr, ev1 = nullptr;
-  cudaEvent_t ev_join[kSideStreams] = {};
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::string err;
   int n = 0;
   std::vector<DevScene> scenes;
-  std::vector<DevMap> maps;
   std::vector<pm_batch_scene> desc;
   std::vector<int> qps;
   std::vector<int64_t> cap, stored, queries;
@@ -50,7 +41,17 @@ struct pm_batch {
   DevBuf raw, keys, counters, status, dropped, rng, slots, srec, res, images;
   DevBuf qka, qkb, qva, qvb, qhist, qcount, qstart, qoff, item_off, knn_counter;
   DevBuf table, offs, err_word, scene_scratch;
-  DevBuf scratch[kSideStreams];
+  // the photon maps of all scenes, built together (batch_maps_launch)
+  struct Shape {
+    int nlevels = 0;
+    int lvl_off[kMaxLevels] = {};
+    int lvl_cnt[kMaxLevels] = {};
+  };
+  std::vector<Shape> shape;
+  std::vector<int64_t> box_base;
+  DevBuf m_pos4, m_thr4, m_wi2, m_boxes, m_keys_b, m_va, m_vb, m_hist, m_bb, m_tab, m_lvl;
+  DevBuf m_order, m_count, m_first, m_sums;
+  BatchMapBuild mb{};
   int64_t total_emit = 0, total_pix = 0, total_slots = 0, total_samples = 0, nq = 0;
   int max_k = 1;
   pm_batch_tuning tune{8, 32, 512, 64, 128, 0};
@@ -62,17 +63,14 @@ struct pm_batch {
   ~pm_batch() {
     if (exec) cudaGraphExecDestroy(exec);
     for (auto& s : scenes) s.release();
-    for (auto& m : maps) m.release();
-    DevBuf* bufs[] = {&raw, &keys, &counters, &status, &dropped, &rng, &slots, &srec, &res,
-                      &images, &qka, &qkb, &qva, &qvb, &qhist, &qcount, &qstart, &qoff,
-                      &item_off, &knn_counter, &table, &offs, &err_word, &scene_scratch};
+    DevBuf* bufs[] = {&raw,    &keys,    &counters, &status, &dropped,  &rng,
+                      &slots,  &srec,    &res,      &images, &qka,      &qkb,
+                      &qva,    &qvb,     &qhist,    &qcount, &qstart,   &qoff,
+                      &item_off, &knn_counter, &table, &offs, &err_word, &scene_scratch,
+                      &m_pos4, &m_thr4,  &m_wi2,    &m_boxes, &m_keys_b, &m_va,
+                      &m_vb,   &m_hist,  &m_bb,     &m_tab,  &m_lvl,    &m_order,
+                      &m_count, &m_first, &m_sums};
     for (DevBuf* b : bufs) b->release();
-    for (auto& b : scratch) b.release();
-    for (int i = 0; i < kSideStreams; ++i) {
-      if (side[i]) cudaStreamDestroy(side[i]);
-      if (ev_join[i]) cudaEventDestroy(ev_join[i]);
-    }
-    if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (st) cudaStreamDestroy(st);
@@ -141,7 +139,18 @@ int upload_tables(pm_batch* b) {
     a.sample_rec = (float4*)b->srec.ptr + b->sample_off[s];
     a.in_rays = nullptr;
     a.err = errw;
-    x.map = map_view(b->maps[s]);
+    MapDev& mv = x.map;
+    const pm_batch::Shape& sh = b->shape.empty() ? pm_batch::Shape{} : b->shape[s];
+    mv.pos4 = (const float4*)b->m_pos4.ptr + b->cap_off[s];
+    mv.thr4 = (const float4*)b->m_thr4.ptr + b->cap_off[s];
+    mv.wi2 = (const float2*)b->m_wi2.ptr + b->cap_off[s];
+    mv.boxes = b->box_base.empty() ? nullptr : (const float4*)b->m_boxes.ptr + 2 * b->box_base[s];
+    mv.n = b->shape.empty() ? 0 : (int)b->stored[s];
+    mv.nlevels = sh.nlevels;
+    for (int l = 0; l < kMaxLevels; ++l) {
+      mv.lvl_off[l] = l < sh.nlevels ? sh.lvl_off[l] : 0;
+      mv.lvl_cnt[l] = l < sh.nlevels ? sh.lvl_cnt[l] : 0;
+    }
     x.k = d.k;
     x.n_emitted = (float)d.n_photons;
     const DevScene& sc = b->scenes[s];
@@ -157,6 +166,7 @@ int upload_tables(pm_batch* b) {
     ta.caustic = 0;
     ta.out = (float*)b->raw.ptr + 9 * b->cap_off[s];
     ta.keys = (unsigned long long*)b->keys.ptr + b->cap_off[s];
+    ta.store_count = (uint32_t*)b->m_count.ptr;  // by the batch's work index
     ta.counter = (unsigned long long*)b->counters.ptr + s;
     ta.cap = (unsigned long long)b->cap[s];
     ta.status = (unsigned*)b->status.ptr;
@@ -211,29 +221,102 @@ void enqueue_trace(pm_batch* b, int block, int stack) {
   batch_trace_launch(b->tables, b->total_emit, block, stack, b->st);
 }
 
-// Orders each scene's photons and builds its map, scenes spread over the
-// side streams (forked from and joined back into the main stream).
-void enqueue_maps(pm_batch* b) {
-  cudaEventRecord(b->ev_fork, b->st);
-  const int ns = std::min(b->n, kSideStreams);
-  for (int i = 0; i < ns; ++i) cudaStreamWaitEvent(b->side[i], b->ev_fork, 0);
-  for (int s = 0; s < b->n; ++s) {
-    const int i = s % kSideStreams;
-    const int m = (int)b->stored[s];
-    DevMap& dm = b->maps[s];
-    if (m > 0) {
-      order_photons_launch((unsigned long long*)b->keys.ptr + b->cap_off[s],
-                           (const float*)b->raw.ptr + 9 * b->cap_off[s], m, 40,
-                           (float*)dm.aos.ptr, b->scratch[i].ptr, b->side[i]);
-      map_build_launch((const float*)dm.aos.ptr, m, (float4*)dm.pos4.ptr, (float4*)dm.thr4.ptr,
-                       (float2*)dm.wi2.ptr, (float4*)dm.boxes.ptr, dm.lvl_off, dm.lvl_cnt,
-                       dm.nlevels, b->scratch[i].ptr, b->side[i]);
+// Orders every scene's photons and builds every scene's map, all scenes
+// in each launch.
+void enqueue_maps(pm_batch* b) { batch_maps_launch(b->mb, b->st); }
+
+int bits_for(int64_t v) {  // smallest b with 2^b >= v
+  int r = 0;
+  while (r < 62 && ((int64_t)1 << r) < v) ++r;
+  return r;
+}
+
+// After the stored counts are known (cap = stored): the map shapes, their
+// device tables and buffers, and the build's arguments.
+int plan_maps(pm_batch* b) {
+  const int n = b->n;
+  const int64_t total = b->cap_off[n];
+  if (total > 0x7fffffffLL)
+    return berr(b, PM_ERR_INVALID_ARGUMENT, "%lld photons stored in the batch (at most 2^31 - 1)",
+                (long long)total);
+  b->shape.assign((size_t)n, pm_batch::Shape{});
+  b->box_base.assign((size_t)n + 1, 0);
+  std::vector<int64_t> group_off((size_t)n + 1, 0), level_off((size_t)kMaxLevels * (n + 1), 0);
+  std::vector<int> lvl((size_t)n * 2 * kMaxLevels, 0);
+  int max_levels = 0;
+  for (int s = 0; s < n; ++s) {
+    pm_batch::Shape& sh = b->shape[s];
+    const int boxes = map_levels(b->stored[s], &sh.nlevels, sh.lvl_off, sh.lvl_cnt);
+    b->box_base[s + 1] = b->box_base[s] + boxes;
+    group_off[s + 1] = group_off[s] + (sh.nlevels > 0 ? sh.lvl_cnt[0] : 0);
+    for (int l = 0; l < kMaxLevels; ++l) {
+      const int cnt = l < sh.nlevels ? sh.lvl_cnt[l] : 0;
+      level_off[(size_t)l * (n + 1) + s + 1] = level_off[(size_t)l * (n + 1) + s] + cnt;
+      lvl[(size_t)s * 2 * kMaxLevels + l] = l < sh.nlevels ? sh.lvl_off[l] : 0;
+      lvl[(size_t)s * 2 * kMaxLevels + kMaxLevels + l] = cnt;
     }
+    max_levels = std::max(max_levels, sh.nlevels);
   }
-  for (int i = 0; i < ns; ++i) {
-    cudaEventRecord(b->ev_join[i], b->side[i]);
-    cudaStreamWaitEvent(b->st, b->ev_join[i], 0);
-  }
+  const size_t tn = (size_t)std::max<int64_t>(total, 1);
+  const size_t nb = (size_t)std::max<int64_t>(b->box_base[n], 1);
+  std::vector<int64_t> tab;
+  tab.insert(tab.end(), b->cap_off.begin(), b->cap_off.end());
+  tab.insert(tab.end(), group_off.begin(), group_off.end());
+  tab.insert(tab.end(), b->box_base.begin(), b->box_base.end());
+  tab.insert(tab.end(), level_off.begin(), level_off.end());
+  tab.insert(tab.end(), b->emit_off.begin(), b->emit_off.end());
+  const size_t te = (size_t)std::max<int64_t>(b->total_emit, 1);
+  int s;
+  if ((s = b->m_pos4.ensure(tn * 16)) || (s = b->m_thr4.ensure(tn * 16)) ||
+      (s = b->m_wi2.ensure(tn * 8)) || (s = b->m_boxes.ensure(nb * 32)) ||
+      (s = b->m_keys_b.ensure(tn * 8)) || (s = b->m_va.ensure(tn * 4)) ||
+      (s = b->m_vb.ensure(tn * 4)) || (s = b->m_order.ensure(tn * 4)) ||
+      (s = b->m_count.ensure(te * 4)) || (s = b->m_first.ensure(te * 4)) ||
+      (s = b->m_sums.ensure((size_t)scan_tiles((int64_t)te) * 4 + 64)) ||
+      (s = b->m_hist.ensure(sort_hist_words((int64_t)tn) * 4)) ||
+      (s = b->m_bb.ensure(24 * (size_t)n)) || (s = b->m_tab.ensure(tab.size() * 8)) ||
+      (s = b->m_lvl.ensure(lvl.size() * 4)))
+    return berr(b, s, "photon maps (%lld photons)", (long long)total);
+  cudaError_t e;
+  if ((e = cudaMemcpyAsync(b->m_tab.ptr, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice,
+                           b->st)) ||
+      (e = cudaMemcpyAsync(b->m_lvl.ptr, lvl.data(), lvl.size() * 4, cudaMemcpyHostToDevice,
+                           b->st)) ||
+      (e = cudaStreamSynchronize(b->st)))
+    return bcuda(b, e, "photon map tables");
+  BatchMapBuild& a = b->mb;
+  a = BatchMapBuild{};
+  const int64_t* t = (const int64_t*)b->m_tab.ptr;
+  a.raw = (const float*)b->raw.ptr;
+  a.keys_a = (unsigned long long*)b->keys.ptr;
+  a.keys_b = (unsigned long long*)b->m_keys_b.ptr;
+  a.va = (uint32_t*)b->m_va.ptr;
+  a.vb = (uint32_t*)b->m_vb.ptr;
+  a.hist = (uint32_t*)b->m_hist.ptr;
+  a.count = (const uint32_t*)b->m_count.ptr;
+  a.first = (uint32_t*)b->m_first.ptr;
+  a.sums = (uint32_t*)b->m_sums.ptr;
+  a.order = (uint32_t*)b->m_order.ptr;
+  a.err = (int*)b->err_word.ptr;
+  a.bb = (uint32_t*)b->m_bb.ptr;
+  a.stored_off = t;
+  a.group_off = t + (n + 1);
+  a.box_base = t + 2 * (n + 1);
+  a.level_off = t + 3 * (n + 1);
+  a.emit_off = t + 3 * (n + 1) + (size_t)kMaxLevels * (n + 1);
+  a.lvl = (const int*)b->m_lvl.ptr;
+  a.pos4 = (float4*)b->m_pos4.ptr;
+  a.thr4 = (float4*)b->m_thr4.ptr;
+  a.wi2 = (float2*)b->m_wi2.ptr;
+  a.boxes = (float4*)b->m_boxes.ptr;
+  a.total = total;
+  a.total_emit = b->total_emit;
+  a.total_groups = group_off[n];
+  for (int l = 0; l < kMaxLevels; ++l) a.level_total[l] = level_off[(size_t)l * (n + 1) + n];
+  a.n_scenes = n;
+  a.scene_bits = bits_for(n);
+  a.max_levels = max_levels;
+  return PM_OK;
 }
 
 void enqueue_camera_and_list(pm_batch* b, int block, int stack) {
@@ -343,25 +426,11 @@ int plan(pm_batch* b) {
     if (!short_cap) break;
     if (attempt == 1) return berr(b, PM_ERR_DEVICE_STATUS, "batch trace: capacity");
   }
-  // 2. photon maps
-  std::vector<size_t> need(kSideStreams, 256);
-  for (int i = 0; i < n; ++i) {
-    DevMap& dm = b->maps[i];
-    const int64_t m = b->stored[i];
-    dm.n = m;
-    const int total = map_levels(m, &dm.nlevels, dm.lvl_off, dm.lvl_cnt);
-    if (m > 0 &&
-        ((s = dm.aos.ensure((size_t)m * 36)) || (s = dm.pos4.ensure((size_t)m * 16)) ||
-         (s = dm.thr4.ensure((size_t)m * 16)) || (s = dm.wi2.ensure((size_t)m * 8)) ||
-         (s = dm.boxes.ensure((size_t)total * 32))))
-      return berr(b, s, "scene %d: photon map (%lld photons)", i, (long long)m);
-    dm.built = true;
-    const size_t sb = std::max(order_scratch_bytes(m), map_build_scratch_bytes(m));
-    need[i % kSideStreams] = std::max(need[i % kSideStreams], sb);
-  }
-  for (int i = 0; i < kSideStreams; ++i)
-    if ((s = b->scratch[i].ensure(need[i])) != PM_OK)
-      return berr(b, s, "map build scratch");
+  // 2. photon maps: the trace regions shrink to the stored counts (the trace
+  // is deterministic), so the stored photons of all scenes lie back to back
+  b->cap = b->stored;
+  if ((s = size_trace(b)) != PM_OK) return s;
+  if ((s = plan_maps(b)) != PM_OK) return s;
   // 3. camera-pass buffers
   const size_t ts = (size_t)std::max<int64_t>(b->total_slots, 2);
   if ((s = b->rng.ensure((size_t)b->total_pix * 8)) ||
@@ -427,24 +496,14 @@ int pm_batch_create(int device, const pm_batch_scene* scenes, int32_t n, pm_batc
   pm_batch* b = new pm_batch();
   b->device = device;
   cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device);
-  cudaError_t e;
-  if ((e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) ||
-      (e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming)) ||
-      (e = cudaEventCreate(&b->ev0)) || (e = cudaEventCreate(&b->ev1))) {
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreate(&b->ev0) != cudaSuccess || cudaEventCreate(&b->ev1) != cudaSuccess) {
     delete b;
     cudaGetLastError();
     return PM_ERR_CUDA;
   }
-  for (int i = 0; i < kSideStreams; ++i)
-    if ((e = cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking)) ||
-        (e = cudaEventCreateWithFlags(&b->ev_join[i], cudaEventDisableTiming))) {
-      delete b;
-      cudaGetLastError();
-      return PM_ERR_CUDA;
-    }
   b->n = n;
   b->scenes.resize((size_t)n);
-  b->maps.resize((size_t)n);
   b->desc.assign(scenes, scenes + n);
   b->qps.assign((size_t)n, 1);
   b->emit_off.assign((size_t)n + 1, 0);
@@ -724,11 +783,19 @@ int pm_batch_photons(pm_batch* b, int32_t scene, float* out) {
   cudaSetDevice(b->device);
   const int64_t m = b->stored[scene];
   if (m == 0) return PM_OK;
+  DevBuf tmp;
+  int s;
+  if ((s = tmp.ensure((size_t)m * 36)) != PM_OK) return berr(b, s, "batch photons");
+  batch_photons_launch((const float*)b->raw.ptr, (const uint32_t*)b->m_order.ptr + b->cap_off[scene],
+                       m, (float*)tmp.ptr, b->st);
   cudaError_t e;
-  if ((e = cudaMemcpyAsync(out, b->maps[scene].aos.ptr, (size_t)m * 36, cudaMemcpyDeviceToHost,
-                           b->st)) ||
-      (e = cudaStreamSynchronize(b->st)))
+  if ((e = cudaGetLastError()) ||
+      (e = cudaMemcpyAsync(out, tmp.ptr, (size_t)m * 36, cudaMemcpyDeviceToHost, b->st)) ||
+      (e = cudaStreamSynchronize(b->st))) {
+    tmp.release();
     return bcuda(b, e, "batch photons");
+  }
+  tmp.release();
   return PM_OK;
 }
 

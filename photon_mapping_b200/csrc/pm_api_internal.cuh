@@ -114,6 +114,7 @@ struct pm_ctx {
   pm::DevScene scene;
   pm::DevBuf dev_err;   // device error word of the kernels (int)
   pm::DevBuf trace_raw, trace_keys, trace_misc;  // photon tracing buffers
+  pm::DevBuf trace_count, trace_first;  // per emitted photon: stores, first index
   pm::DevBuf r_rng, r_accum, r_slots, r_srec, r_res, r_sort, r_misc;  // render
   pm::DevBuf r_shadow;  // FP64 per-pixel sums of PM_RENDER_FP64_CHECK
   pm::DevBuf scratch;  // map build scratch
@@ -144,6 +145,8 @@ struct pm_ctx {
     trace_raw.release();
     trace_keys.release();
     trace_misc.release();
+    trace_count.release();
+    trace_first.release();
     r_rng.release(); r_accum.release(); r_slots.release(); r_srec.release();
     r_res.release(); r_sort.release(); r_misc.release(); r_shadow.release();
     diff.release();

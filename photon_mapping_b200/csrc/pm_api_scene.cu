@@ -142,6 +142,9 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
       for (int i = 0; i < 3; ++i) cudaEventDestroy(ev[i]);
     }
   } guard{ev};
+  const size_t ne = (size_t)(n_emit > 0 ? n_emit : 1);
+  if ((s = c->trace_count.ensure(ne * 4)) != PM_OK)
+    return set_err(c, s, "trace buffers (%lld photons)", (long long)n_emit);
   for (int attempt = 0; attempt < 2; ++attempt) {
     if ((s = c->trace_raw.ensure(cap * 36)) || (s = c->trace_keys.ensure(cap * 8)))
       return set_err(c, s, "trace buffers (%llu photons)", cap);
@@ -154,6 +157,7 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
     a.caustic = map == PM_MAP_CAUSTICS;
     a.out = (float*)c->trace_raw.ptr;
     a.keys = (unsigned long long*)c->trace_keys.ptr;
+    a.store_count = (uint32_t*)c->trace_count.ptr;
     a.counter = counter;
     a.cap = cap;
     a.status = status;
@@ -178,17 +182,16 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
     return set_err(c, PM_ERR_INVALID_ARGUMENT, "%llu photons stored", stored);
   DevMap& dm = c->maps[map];
   const int n = (int)stored;
-  if (first && (s = first->ensure((size_t)(n_emit > 0 ? n_emit : 1) * 4)) != PM_OK)
-    return set_err(c, s, "photon offsets");
+  DevBuf* fb = first ? first : &c->trace_first;
+  if ((s = fb->ensure(ne * 4)) != PM_OK) return set_err(c, s, "photon offsets");
   if (n > 0) {
     if ((s = dm.aos.ensure((size_t)n * 36)) ||
-        (s = c->scratch.ensure(order_scratch_bytes(n))))
+        (s = c->scratch.ensure(order_scratch_bytes(n_emit))))
       return set_err(c, s, "photon order buffers");
-    // photon index < 2^31, bounce < 2^8: 39-bit keys
-    order_photons_launch((unsigned long long*)c->trace_keys.ptr,
-                         (const float*)c->trace_raw.ptr, n, 40,
-                         (float*)dm.aos.ptr, c->scratch.ptr, st,
-                         first ? (uint32_t*)first->ptr : nullptr);
+    order_photons_launch((const unsigned long long*)c->trace_keys.ptr,
+                         (const float*)c->trace_raw.ptr, n, (const uint32_t*)c->trace_count.ptr,
+                         n_emit, (uint32_t*)fb->ptr, (float*)dm.aos.ptr, c->scratch.ptr,
+                         (int*)c->dev_err.ptr, st);
     if ((e = cudaGetLastError()) != cudaSuccess)
       return cuda_status(c, e, "photon order");
   }
@@ -196,6 +199,7 @@ int trace_map(pm_ctx* c, int map, uint64_t seed, int64_t n_emit, int max_depth,
   cudaEventRecord(ev[2], st);
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess)
     return cuda_status(c, e, "photon map build");
+  if ((s = take_device_error(c, "photon order")) != PM_OK) return s;
   c->map_emitted[map] = n_emit;
   if (stats) {
     stats->emitted = n_emit;

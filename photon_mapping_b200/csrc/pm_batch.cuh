@@ -62,6 +62,51 @@ struct BatchTables {
 void batch_trace_launch(const BatchTables& t, int64_t total_emit, int block, int stack,
                         cudaStream_t st);
 
+// The photon maps of every scene of a batch (pm_batch_maps.cu). The trace
+// wrote scene s's stored photons and their keys (photon << 8 | ordinal) to
+// records [stored_off[s], stored_off[s + 1]) of raw / keys_a, and the store
+// count of the photon with work index emit_off[s] + p to count. order
+// receives, for each scene's index-order places (at the same offsets), the
+// trace record there; the map goes to pos4 / thr4 / wi2 at the same
+// offsets and the boxes from box 2 * box_base[s] on. All device arrays.
+struct BatchMapBuild {
+  const float* raw;                 // total records of 9 floats
+  unsigned long long* keys_a;       // total: the trace's keys, then sort scratch
+  unsigned long long* keys_b;       // total: map keys
+  uint32_t* va;                     // total each: sort values
+  uint32_t* vb;
+  uint32_t* hist;                   // sort_hist_words(total)
+  const uint32_t* count;            // total_emit
+  uint32_t* first;                  // total_emit: first index of each photon's stores
+  uint32_t* sums;                   // scan_tiles(total_emit)
+  uint32_t* order;                  // total
+  uint32_t* bb;                     // 6 n: the scenes' position boxes
+  int* err;                         // device error word
+  const int64_t* stored_off;        // n + 1
+  const int64_t* emit_off;          // n + 1
+  const int64_t* group_off;         // n + 1: prefix of the 8-photon groups
+  const int64_t* box_base;          // n
+  const int64_t* level_off;         // kMaxLevels rows of n + 1: prefix of level-l boxes
+  const int* lvl;                   // n x (kMaxLevels level offsets, kMaxLevels counts)
+  float4* pos4;
+  float4* thr4;
+  float2* wi2;
+  float4* boxes;
+  int64_t total;                    // stored photons of all scenes (< 2^31)
+  int64_t total_emit;
+  int64_t total_groups;
+  int64_t level_total[kMaxLevels];  // boxes of level l over all scenes
+  int n_scenes;
+  int scene_bits;   // bits of a scene number
+  int max_levels;   // most tree levels of any scene
+};
+
+void batch_maps_launch(const BatchMapBuild& a, cudaStream_t st);
+
+// out[j] = raw record order[j], j < m (9 floats each).
+void batch_photons_launch(const float* raw, const uint32_t* order, int64_t m, float* out,
+                          cudaStream_t st);
+
 // Camera pass of every pixel of every scene (pm_render.cu): sampler seeds,
 // then the camera kernel.
 void batch_camera_launch(const BatchTables& t, int64_t total_pix, int block, int stack,

@@ -36,7 +36,7 @@ __host__ __device__ unsigned long long photon_stream_state(
 }
 
 __device__ __forceinline__ void store_photon(const TraceArgs& a, int photon,
-                                             int bounce, V3 thr, V3 pos,
+                                             int ordinal, V3 thr, V3 pos,
                                              V3 wi) {
   const unsigned long long slot = atomicAdd(a.counter, 1ull);
   if (slot >= a.cap) return;
@@ -44,7 +44,7 @@ __device__ __forceinline__ void store_photon(const TraceArgs& a, int photon,
   o[0] = thr.x; o[1] = thr.y; o[2] = thr.z;
   o[3] = pos.x; o[4] = pos.y; o[5] = pos.z;
   o[6] = wi.x; o[7] = wi.y; o[8] = wi.z;
-  a.keys[slot] = ((unsigned long long)photon << 8) | (unsigned)bounce;
+  a.keys[slot] = ((unsigned long long)photon << 8) | (unsigned)ordinal;
 }
 
 enum { kTracePlain = 0, kTraceFrozen = 1, kTraceReplay = 2 };
@@ -63,7 +63,7 @@ struct PhotonPath {
   V3 org, dir;
   int i;          // photon index within its map
   int k;          // bounce
-  int nst;        // photons stored so far (replay)
+  int nst;        // photons stored so far
   bool prev_specular;
 };
 
@@ -146,7 +146,7 @@ __device__ __forceinline__ bool photon_step(const SceneDev& sc, const TraceArgs&
         }
       }
     } else {
-      store_photon(a, p.i, p.k, p.thr, s.pos, -p.dir);
+      store_photon(a, p.i, p.nst, p.thr, s.pos, -p.dir);
     }
     ++p.nst;
   }
@@ -199,6 +199,7 @@ __device__ __forceinline__ void trace_persistent(unsigned long long* next, long 
   const int lane = (int)(threadIdx.x & 31);
   PhotonPath p;
   int src = 0;
+  long long g = 0;  // work index of the current path
   bool live = false, done = false;
   unsigned nrays = 0;  // closest-hit queries of this thread
   while (true) {
@@ -209,9 +210,9 @@ __device__ __forceinline__ void trace_persistent(unsigned long long* next, long 
       if (lane == leader) base = atomicAdd(next, (unsigned long long)__popc(want));
       base = __shfl_sync(kFull, base, leader);
       if (!live && !done) {
-        const unsigned long long g = base + (unsigned)__popc(want & lanemask_lt());
-        if ((long long)g < total) {
-          const int i = first((long long)g, src);
+        g = (long long)(base + (unsigned)__popc(want & lanemask_lt()));
+        if (g < total) {
+          const int i = first(g, src);
           photon_emit<MODE>(scene(src), args(src), i, p);
           if (MODE == kTraceReplay)
             for (int j = 0; j < args(src).n_params; ++j) rs->cnt[j][threadIdx.x] = 0;
@@ -222,7 +223,13 @@ __device__ __forceinline__ void trace_persistent(unsigned long long* next, long 
       }
     }
     if (__ballot_sync(kFull, live) == 0) break;
-    if (live) live = photon_step<MODE, STACK>(scene(src), args(src), p, rs, nrays);
+    if (live) {
+      live = photon_step<MODE, STACK>(scene(src), args(src), p, rs, nrays);
+      if (!live && MODE != kTraceReplay) {
+        uint32_t* sc = args(src).store_count;
+        if (sc) sc[g] = (uint32_t)p.nst;
+      }
+    }
   }
   unsigned long long* rays = args(0).rays;
   if (rays) {
@@ -251,17 +258,6 @@ __global__ void __launch_bounds__(128)
     return;
   }
   trace_persistent<MODE, kBvhStack>(a.next, a.n_emit, nullptr, scene, args, first);
-}
-
-__global__ void gather_photons_kernel(const float* __restrict__ raw,
-                                      const uint32_t* __restrict__ order,
-                                      int n, float* __restrict__ out) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const float* r = raw + 9 * (size_t)order[s];
-  float* o = out + 9 * (size_t)s;
-#pragma unroll
-  for (int j = 0; j < 9; ++j) o[j] = r[j];
 }
 
 // Every emitted photon of every scene of a batch: the global map rule, each
@@ -302,20 +298,6 @@ void batch_trace_launch(const BatchTables& t, int64_t total_emit, int block, int
     batch_trace_kernel<64><<<gb, block, 0, st>>>(t, total_emit);
 }
 
-// first[p] = sorted index of the first stored photon of emitted photon p.
-__global__ void first_of_photon_kernel(const unsigned long long* __restrict__ keys,
-                                       int n, uint32_t* __restrict__ first) {
-  const int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s >= n) return;
-  const unsigned long long p = keys[s] >> 8;
-  if (s == 0 || (keys[s - 1] >> 8) != p) first[p] = (uint32_t)s;
-}
-
-__global__ void iota_kernel(uint32_t* v, int n) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) v[i] = (uint32_t)i;
-}
-
 void trace_launch(const SceneDev& sc, const TraceArgs& a, cudaStream_t st) {
   if (a.n_emit <= 0) return;
   const int tb = 128;  // ReplaySmem holds 128 threads' counters
@@ -331,26 +313,39 @@ void trace_launch(const SceneDev& sc, const TraceArgs& a, cudaStream_t st) {
     trace_kernel<kTracePlain><<<gb, tb, 0, st>>>(sc, a);
 }
 
-size_t order_scratch_bytes(int64_t n) {
-  const size_t nn = (size_t)(n > 1 ? n : 2);
-  return 2 * nn * 8 + 2 * nn * 4 + sort_hist_words(nn) * 4 + 64;
+// out[first[p] + j] = the record with key p << 8 | j.
+__global__ void rank_scatter_kernel(const unsigned long long* __restrict__ keys,
+                                    const float* __restrict__ raw, int64_t n,
+                                    const uint32_t* __restrict__ first, float* __restrict__ out,
+                                    int* __restrict__ err) {
+  for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long key = keys[r];
+    const int64_t d = (int64_t)first[key >> 8] + (int64_t)(key & 255u);
+    if (d >= n) {
+      atomicOr(err, 32);
+      continue;
+    }
+    const float* src = raw + 9 * r;
+    float* dst = out + 9 * d;
+#pragma unroll
+    for (int q = 0; q < 9; ++q) dst[q] = src[q];
+  }
 }
 
-void order_photons_launch(unsigned long long* keys, const float* raw, int n,
-                          int key_bits, float* out, void* scratch,
-                          cudaStream_t st, uint32_t* first) {
-  if (n <= 0) return;
-  unsigned long long* kb = (unsigned long long*)scratch;
-  uint32_t* va = (uint32_t*)(kb + n);
-  uint32_t* vb = va + n;
-  uint32_t* hist = vb + n;
+size_t order_scratch_bytes(int64_t n_emit) {
+  return (size_t)scan_tiles(n_emit > 1 ? n_emit : 1) * 4 + 64;
+}
+
+void order_photons_launch(const unsigned long long* keys, const float* raw, int64_t n,
+                          const uint32_t* count, int64_t n_emit, uint32_t* first, float* out,
+                          void* scratch, int* err, cudaStream_t st) {
+  if (n <= 0 || n_emit <= 0) return;
+  uint32_t* sums = (uint32_t*)scratch;
+  exclusive_scan_u32(count, first, n_emit, sums, st);
   const int tb = 256;
-  const int gb = (n + tb - 1) / tb;
-  iota_kernel<<<gb, tb, 0, st>>>(va, n);
-  const bool in_b = radix_sort_pairs<unsigned long long>(keys, va, kb, vb, n,
-                                                          key_bits, hist, st);
-  gather_photons_kernel<<<gb, tb, 0, st>>>(raw, in_b ? vb : va, n, out);
-  if (first) first_of_photon_kernel<<<gb, tb, 0, st>>>(in_b ? kb : keys, n, first);
+  const int64_t gb = std::min<int64_t>((n + tb - 1) / tb, (int64_t)sm_count() * 16);
+  rank_scatter_kernel<<<(unsigned)gb, tb, 0, st>>>(keys, raw, n, first, out, err);
 }
 
 }  // namespace pm

@@ -14,7 +14,11 @@ struct TraceArgs {
   int max_depth;  // bounces (<= 255)
   int caustic;    // 0: global map rule, 1: caustics map rule
   float* out;     // 9 floats per stored photon (append order)
-  unsigned long long* keys;     // (photon index << 8 | bounce) per photon
+  unsigned long long* keys;     // (photon index << 8 | j) per stored photon, j its
+                                // ordinal among its photon's stores (< 255)
+  uint32_t* store_count;        // per work index of the launch (the photon index
+                                // of a single trace): photons its path stored,
+                                // written when the path ends; or null
   unsigned long long* counter;  // photons stored (keeps counting past cap)
   unsigned long long cap;       // capacity of out / keys
   unsigned* status;  // [0] NaN throughput, [1] negative throughput
@@ -44,14 +48,17 @@ __host__ __device__ unsigned long long photon_stream_state(
 
 void trace_launch(const SceneDev& sc, const TraceArgs& a, cudaStream_t st);
 
-size_t order_scratch_bytes(int64_t n);
-
-// Sorts the n appended photons by key (key_bits wide) into `out`. With
-// first != null, first[p] receives the sorted index of the first stored
-// photon of emitted photon p (entries of photons that stored none are left
-// as they were).
-void order_photons_launch(unsigned long long* keys, const float* raw, int n,
-                          int key_bits, float* out, void* scratch,
-                          cudaStream_t st, uint32_t* first = nullptr);
+// The n appended photons of a trace of n_emit photons, in index order (the
+// order PhotonMapping::build appends them to its photon vector,
+// integrator.h:406-469): photon p's stores come after every store of the
+// photons before it, in path order. With the store counts the trace wrote,
+// first[p] = count[0] + ... + count[p - 1] (an exclusive scan) is the index
+// of p's first stored photon, and the record with key p << 8 | j goes to
+// out[first[p] + j]: no sort. A key whose index falls outside [0, n) sets
+// bit 5 (32) of *err and is dropped. scratch: order_scratch_bytes(n_emit).
+size_t order_scratch_bytes(int64_t n_emit);
+void order_photons_launch(const unsigned long long* keys, const float* raw, int64_t n,
+                          const uint32_t* count, int64_t n_emit, uint32_t* first, float* out,
+                          void* scratch, int* err, cudaStream_t st);
 
 }  // namespace pm
