@@ -185,7 +185,7 @@ typedef struct pm_material {
 } pm_material;
 
 /* Replaces Scene::build (scene.h:275-304): uploads the faces and builds the
- * device LBVH. vertices and normals hold 9 floats per face (the reference's
+ * device BVH. vertices and normals hold 9 floats per face (the reference's
  * per-face unshared vertices, scene.h:199-212; a face without normals
  * carries its geometric normal three times, scene.h:182-189). */
 int pm_scene_upload(pm_ctx* ctx, const float* vertices, const float* normals,
@@ -426,12 +426,12 @@ typedef struct pm_batch_tuning {
   int32_t knn_warps;   /* warps per block of the persistent kNN kernel, 1..8 */
   int32_t knn_chunk;   /* consecutive queries per warp work item, 1..1024    */
   int32_t knn_buffer;  /* candidate buffer per warp: 512 (k <= 224) or 2048  */
-  int32_t bvh_stack;   /* BVH traversal stack entries: 32 or 64              */
+  int32_t bvh_stack;   /* BVH traversal stack entries: 16, 32 or 64          */
   int32_t block;       /* threads per block of trace and camera: 64..256     */
   int32_t reserved;
 } pm_batch_tuning;
 
-/* Uploads every scene (its own LBVH), sizes every buffer by running the
+/* Uploads every scene (its own BVH), sizes every buffer by running the
  * step once (photons stored and queries per scene), and keeps the scenes'
  * parameters. */
 int pm_batch_create(int device, const pm_batch_scene* scenes, int32_t n_scenes,

@@ -1,6 +1,6 @@
 // Drop-in for the reference's scene.h (scene.h:53-356): Scene with
 // loadModel (OBJ + MTL, the reference loader's rules), build (upload and
-// device LBVH through pm_scene_upload) and intersect (pm_scene_intersect;
+// device BVH through pm_scene_upload) and intersect (pm_scene_intersect;
 // the surface frame is filled on the host as scene.h:324-343 does).
 #ifndef PM_DROPIN_SCENE_H
 #define PM_DROPIN_SCENE_H

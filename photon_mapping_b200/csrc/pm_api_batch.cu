@@ -105,7 +105,7 @@ int key_bits(int n_scenes) {
 bool tuning_ok(const pm_batch* b, const pm_batch_tuning& t) {
   return t.knn_warps >= 1 && t.knn_warps <= 8 && t.knn_chunk >= 1 && t.knn_chunk <= 1024 &&
          (t.knn_buffer == 2048 || (t.knn_buffer == 512 && b->max_k <= 224)) &&
-         (t.bvh_stack == 32 || t.bvh_stack == 64) && t.block >= 64 && t.block <= 256 &&
+         (t.bvh_stack == 16 || t.bvh_stack == 32 || t.bvh_stack == 64) && t.block >= 64 && t.block <= 256 &&
          t.block % 32 == 0;
 }
 
@@ -657,7 +657,7 @@ int pm_batch_autotune(pm_batch* b, pm_batch_tuning* best, float* ms_stage) {
   // trace and camera: block x stack
   float best_tc = 3.4e38f, best_trace = 0.f, best_cam = 0.f;
   const int blocks[] = {64, 128, 256};
-  const int stacks[] = {32, 64};
+  const int stacks[] = {16, 32, 64};
   for (int bl : blocks)
     for (int sk : stacks) {
       float tt = 0.f, tc = 0.f;

@@ -161,7 +161,7 @@ MapDev map_view(const DevMap& dm);
 int build_map(pm_ctx* c, DevMap& dm, const float* d_aos, int64_t n,
               cudaStream_t st);
 int take_device_error(pm_ctx* c, const char* where);
-// Uploads a scene and builds its LBVH on stream st (synchronises st). On
+// Uploads a scene and builds its BVH on stream st (synchronises st). On
 // failure returns the status and names the step in *what.
 int upload_scene(DevScene& sc, DevBuf& scratch, cudaStream_t st, const float* vertices,
                  const float* normals, const pm_material* materials, int64_t n,

@@ -101,11 +101,14 @@ int upload_scene(DevScene& sc, DevBuf& scratch, cudaStream_t st, const float* ve
        (e = cudaMemcpyAsync(sc.lights.ptr, lights.data(), lights.size() * 4,
                             cudaMemcpyHostToDevice, st))))
     return e == cudaErrorMemoryAllocation ? PM_ERR_OUT_OF_MEMORY : PM_ERR_CUDA;
-  scene_build_launch((const float*)sc.verts_in.ptr, (const float*)sc.nrms_in.ptr,
-                     (int)n, (float4*)sc.tri.ptr, (float4*)sc.nrm.ptr,
-                     (float4*)sc.geo.ptr, (float4*)sc.mt.ptr,
-                     (float4*)sc.nodes.ptr, scratch.ptr, st);
   *what = "scene build";
+  if ((e = scene_build_launch((const float*)sc.verts_in.ptr, (const float*)sc.nrms_in.ptr,
+                              (int)n, (float4*)sc.tri.ptr, (float4*)sc.nrm.ptr,
+                              (float4*)sc.geo.ptr, (float4*)sc.mt.ptr, (float4*)sc.nodes.ptr,
+                              scratch.ptr, st)) != cudaSuccess) {
+    cudaGetLastError();
+    return e == cudaErrorMemoryAllocation ? PM_ERR_OUT_OF_MEMORY : PM_ERR_CUDA;
+  }
   if ((e = cudaGetLastError()) != cudaSuccess) return PM_ERR_CUDA;
   if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return PM_ERR_CUDA;
   sc.built = true;

@@ -506,7 +506,9 @@ void batch_camera_launch(const BatchTables& t, int64_t total_pix, int block, int
                          cudaStream_t st) {
   if (total_pix <= 0) return;
   const unsigned gb = (unsigned)((total_pix + block - 1) / block);
-  if (stack <= 32)
+  if (stack <= 16)
+    batch_camera_kernel<16><<<gb, block, 0, st>>>(t, total_pix);
+  else if (stack <= 32)
     batch_camera_kernel<32><<<gb, block, 0, st>>>(t, total_pix);
   else
     batch_camera_kernel<64><<<gb, block, 0, st>>>(t, total_pix);

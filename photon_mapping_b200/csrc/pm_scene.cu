@@ -1,12 +1,14 @@
-// Scene upload and LBVH build on the device (replaces the Embree BVH of
+// Scene upload and BVH build on the device (replaces the Embree BVH of
 // scene.h:275-304): per-face constants, Morton codes of the triangle
-// centroids, radix sort, the binary radix tree of Karras (2012) over the
-// sorted codes, and a bottom-up refit of padded child boxes.
+// centroids, radix sort, then the tree built by parallel locally-ordered
+// clustering over the sorted leaves (PLOC, below).
 #include "pm_scene.cuh"
 #include "pm_scene_build.cuh"
 #include "pm_sort.cuh"
 
 #include <float.h>
+
+#include <utility>
 
 namespace pm {
 
@@ -96,59 +98,40 @@ __global__ void leaf_setup_kernel(const float4* __restrict__ tri, int n,
   mt[3 * i + 2] = make_float4(e2.x, e2.y, e2.z, 0.f);
 }
 
-// Length of the common prefix of (code, index) pairs i and j; -1 outside.
-__device__ __forceinline__ int delta(const uint32_t* __restrict__ codes, int n,
-                                     int i, int j) {
-  if (j < 0 || j >= n) return -1;
-  const uint32_t a = codes[i], b = codes[j];
-  if (a != b) return __clz(a ^ b);
-  return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+// ------------------------------------------------------------ BVH (PLOC)
+//
+// Parallel locally-ordered clustering (Meister & Bittner, IEEE TVCG 2018):
+// the clusters start as the leaves in Morton order; each pass finds every
+// cluster's nearest neighbour among the kPlocRadius clusters on either side
+// (the distance is the surface area of the two boxes' union), merges every
+// mutual pair into a new internal node and compacts the clusters in order.
+// Pairs are ordered by (union area, index distance, parity of the smaller
+// index, smaller index): a total order on pairs, so the globally first pair
+// is mutual and every pass merges at least one pair, and clusters with
+// equal boxes pair up as (2k, 2k + 1), a balanced tree, instead of all
+// choosing one neighbour (a chain one merge per pass). Internal nodes are
+// numbered from the top down in creation order (the last merge, the root,
+// is node 0). Leaf boxes are padded by `pad`, so ray/box rounding never
+// culls a hit triangle; a parent's box is the union of its children's.
+
+constexpr int kPlocRadius = 16;
+constexpr int kPlocBlock = 256;
+
+__device__ __forceinline__ float union_area(float4 alo, float4 ahi, float4 blo, float4 bhi) {
+  const float dx = fmaxf(ahi.x, bhi.x) - fminf(alo.x, blo.x);
+  const float dy = fmaxf(ahi.y, bhi.y) - fminf(alo.y, blo.y);
+  const float dz = fmaxf(ahi.z, bhi.z) - fminf(alo.z, blo.z);
+  const float a = dx * dy + dy * dz + dz * dx;
+  return a <= FLT_MAX ? a : FLT_MAX;  // NaN and infinity order last
 }
 
-// Karras 2012: internal node i of the binary radix tree over n sorted
-// codes. Children: >= 0 internal node, < 0 leaf ~index.
-__global__ void radix_tree_kernel(const uint32_t* __restrict__ codes, int n,
-                                  int* __restrict__ child,
-                                  int* __restrict__ parent) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n - 1) return;
-  const int d = (delta(codes, n, i, i + 1) - delta(codes, n, i, i - 1)) >= 0 ? 1 : -1;
-  const int dmin = delta(codes, n, i, i - d);
-  int lmax = 2;
-  while (delta(codes, n, i, i + lmax * d) > dmin) lmax *= 2;
-  int l = 0;
-  for (int t = lmax / 2; t >= 1; t /= 2)
-    if (delta(codes, n, i, i + (l + t) * d) > dmin) l += t;
-  const int j = i + l * d;
-  const int dnode = delta(codes, n, i, j);
-  int s = 0;
-  for (int div = 2;; div *= 2) {
-    const int t = (l + div - 1) / div;
-    if (delta(codes, n, i, i + (s + t) * d) > dnode) s += t;
-    if (t == 1) break;
-  }
-  const int g = i + s * d + min(d, 0);
-  const int left = (min(i, j) == g) ? ~g : g;
-  const int right = (max(i, j) == g + 1) ? ~(g + 1) : g + 1;
-  child[2 * i] = left;
-  child[2 * i + 1] = right;
-  // parents: internal nodes in [0, n-1), leaves at n-1 + leaf
-  parent[left < 0 ? (n - 1 + ~left) : left] = i;
-  parent[right < 0 ? (n - 1 + ~right) : right] = i;
-}
-
-// Bottom-up refit: each leaf walks towards the root; the second child to
-// arrive at a node merges both child boxes and continues. Boxes are padded
-// by `pad` so ray/box rounding never culls a hit triangle.
-__global__ void refit_kernel(const float4* __restrict__ mt, int n,
-                             const int* __restrict__ child,
-                             const int* __restrict__ parent,
-                             unsigned* __restrict__ flags,
-                             float4* __restrict__ nodes,
-                             const uint32_t* __restrict__ bb) {
+// Leaf clusters: id ~leaf, box of the leaf triangle padded by 4e-5 of the
+// scene's size (largest extent or coordinate).
+__global__ void ploc_leaf_kernel(const float4* __restrict__ mt, int n,
+                                 const uint32_t* __restrict__ bb, int* __restrict__ cid,
+                                 float4* __restrict__ blo, float4* __restrict__ bhi) {
   const int leaf = blockIdx.x * blockDim.x + threadIdx.x;
   if (leaf >= n) return;
-  // padding: 4e-5 of the scene's size (largest extent or coordinate)
   float size = 0.f;
   for (int a = 0; a < 3; ++a) {
     const float lo = from_ordered(bb[a]), hi = from_ordered(bb[3 + a]);
@@ -158,61 +141,136 @@ __global__ void refit_kernel(const float4* __restrict__ mt, int n,
   const V3 p0 = f4v3(mt[3 * leaf]);
   const V3 p1 = p0 + f4v3(mt[3 * leaf + 1]);
   const V3 p2 = p0 + f4v3(mt[3 * leaf + 2]);
-  float4 lo = make_float4(fminf(fminf(p0.x, p1.x), p2.x) - pad,
+  blo[leaf] = make_float4(fminf(fminf(p0.x, p1.x), p2.x) - pad,
                           fminf(fminf(p0.y, p1.y), p2.y) - pad,
                           fminf(fminf(p0.z, p1.z), p2.z) - pad, 0.f);
-  float4 hi = make_float4(fmaxf(fmaxf(p0.x, p1.x), p2.x) + pad,
+  bhi[leaf] = make_float4(fmaxf(fmaxf(p0.x, p1.x), p2.x) + pad,
                           fmaxf(fmaxf(p0.y, p1.y), p2.y) + pad,
                           fmaxf(fmaxf(p0.z, p1.z), p2.z) + pad, 0.f);
-  int me = ~leaf;
-  int node = parent[n - 1 + leaf];
-  // at most n - 1 steps up
-  for (int step = 0; step < n; ++step) {
-    const bool is_left = child[2 * node] == me;
-    float4* slot = nodes + 4 * node + (is_left ? 0 : 2);
-    slot[0] = make_float4(lo.x, lo.y, lo.z, __int_as_float(child[2 * node]));
-    slot[1] = make_float4(hi.x, hi.y, hi.z, __int_as_float(child[2 * node + 1]));
-    if (!is_left) {
-      // keep the child ids in the node's first two words
-      nodes[4 * node].w = __int_as_float(child[2 * node]);
-      nodes[4 * node + 1].w = __int_as_float(child[2 * node + 1]);
+  cid[leaf] = ~leaf;
+}
+
+// nn[i] = the cluster j != i, |i - j| <= kPlocRadius, whose pair with i
+// comes first in the pair order. m >= 2.
+__global__ void __launch_bounds__(kPlocBlock)
+    ploc_nn_kernel(const float4* __restrict__ blo, const float4* __restrict__ bhi, int m,
+                   int* __restrict__ nn) {
+  __shared__ float4 slo[kPlocBlock + 2 * kPlocRadius];
+  __shared__ float4 shi[kPlocBlock + 2 * kPlocRadius];
+  const int base = blockIdx.x * kPlocBlock - kPlocRadius;
+  for (int t = threadIdx.x; t < kPlocBlock + 2 * kPlocRadius; t += blockDim.x) {
+    const int k = base + t;
+    if (k >= 0 && k < m) {
+      slo[t] = blo[k];
+      shi[t] = bhi[k];
     }
-    __threadfence();
-    if (atomicAdd(&flags[node], 1u) == 0) return;
-    __threadfence();
-    const volatile float4* vn = nodes + 4 * node;
-    const float4 a = make_float4(vn[0].x, vn[0].y, vn[0].z, 0.f);
-    const float4 b = make_float4(vn[1].x, vn[1].y, vn[1].z, 0.f);
-    const float4 c = make_float4(vn[2].x, vn[2].y, vn[2].z, 0.f);
-    const float4 e = make_float4(vn[3].x, vn[3].y, vn[3].z, 0.f);
-    lo = make_float4(fminf(a.x, c.x), fminf(a.y, c.y), fminf(a.z, c.z), 0.f);
-    hi = make_float4(fmaxf(b.x, e.x), fmaxf(b.y, e.y), fmaxf(b.z, e.z), 0.f);
-    if (node == 0) return;
-    me = node;
-    node = parent[node];
   }
+  __syncthreads();
+  const int i = blockIdx.x * kPlocBlock + threadIdx.x;
+  if (i >= m) return;
+  const float4 lo = slo[threadIdx.x + kPlocRadius], hi = shi[threadIdx.x + kPlocRadius];
+  float best = INFINITY;
+  int bj = -1, bkey = 0;
+  for (int o = -kPlocRadius; o <= kPlocRadius; ++o) {
+    const int j = i + o;
+    if (o == 0 || j < 0 || j >= m) continue;
+    const int t = threadIdx.x + kPlocRadius + o;
+    const float c = union_area(lo, hi, slo[t], shi[t]);
+    // ties: nearer first, then an even smaller index, then the smaller one
+    const int mn = min(i, j);
+    const int key = (abs(o) << 2) | ((mn & 1) << 1) | (o > 0 ? 1 : 0);
+    if (c < best || (c == best && key < bkey)) {
+      best = c;
+      bj = j;
+      bkey = key;
+    }
+  }
+  nn[i] = bj;
+}
+
+// mflag[i]: i merges with nn[i] and owns the new node (mutual, i < nn[i]);
+// keep[i]: cluster i survives the pass (not absorbed by a smaller owner).
+__global__ void ploc_flags_kernel(const int* __restrict__ nn, int m, uint32_t* __restrict__ mflag,
+                                  uint32_t* __restrict__ keep) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  const int j = nn[i];
+  const bool mutual = nn[j] == i;
+  mflag[i] = mutual && i < j;
+  keep[i] = !(mutual && j < i);
+}
+
+// The pass's merges and the compacted clusters. Merge owner i gets node
+// top - 1 - mrank[i]; out[0] = clusters left, out[1] = merges.
+__global__ void ploc_merge_kernel(const int* __restrict__ cid, const float4* __restrict__ blo,
+                                  const float4* __restrict__ bhi, const int* __restrict__ nn,
+                                  int m, const uint32_t* __restrict__ mflag,
+                                  const uint32_t* __restrict__ mrank,
+                                  const uint32_t* __restrict__ keep,
+                                  const uint32_t* __restrict__ kpos, int top,
+                                  int* __restrict__ cid2, float4* __restrict__ blo2,
+                                  float4* __restrict__ bhi2, float4* __restrict__ nodes,
+                                  int* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  if (i == m - 1) {
+    out[0] = (int)(kpos[i] + keep[i]);
+    out[1] = (int)(mrank[i] + mflag[i]);
+  }
+  if (!keep[i]) return;
+  const float4 alo = blo[i], ahi = bhi[i];
+  const int o = (int)kpos[i];
+  if (!mflag[i]) {
+    cid2[o] = cid[i];
+    blo2[o] = alo;
+    bhi2[o] = ahi;
+    return;
+  }
+  const int j = nn[i];
+  const float4 clo = blo[j], chi = bhi[j];
+  const int idx = top - 1 - (int)mrank[i];
+  float4* nd = nodes + 4 * (size_t)idx;
+  nd[0] = make_float4(alo.x, alo.y, alo.z, __int_as_float(cid[i]));
+  nd[1] = make_float4(ahi.x, ahi.y, ahi.z, __int_as_float(cid[j]));
+  nd[2] = make_float4(clo.x, clo.y, clo.z, 0.f);
+  nd[3] = make_float4(chi.x, chi.y, chi.z, 0.f);
+  cid2[o] = idx;
+  blo2[o] = make_float4(fminf(alo.x, clo.x), fminf(alo.y, clo.y), fminf(alo.z, clo.z), 0.f);
+  bhi2[o] = make_float4(fmaxf(ahi.x, chi.x), fmaxf(ahi.y, chi.y), fmaxf(ahi.z, chi.z), 0.f);
 }
 
 size_t scene_build_scratch_bytes(int n) {
   const size_t nn = (size_t)(n > 1 ? n : 2);
-  // keys a/b, vals a/b, hist, bbox, child (2n), parent (2n), flags (n)
-  return 4 * nn * 4 + sort_hist_words(nn) * 4 + 64 + 2 * nn * 4 +
-         2 * nn * 4 + nn * 4;
+  // cluster boxes a/b (4n float4), sort keys / values a/b (4n), histogram,
+  // scene box, cluster ids a/b and neighbours (3n), pass flags and ranks
+  // (4n), scan tile sums, pass counts
+  return 4 * nn * 16 + 4 * nn * 4 + sort_hist_words(nn) * 4 + 64 + 3 * nn * 4 + 4 * nn * 4 +
+         (size_t)scan_tiles((int64_t)nn) * 4 + 64;
 }
 
-void scene_build_launch(const float* verts, const float* nrms, int n,
-                        float4* tri, float4* nrm, float4* geo, float4* mt,
-                        float4* nodes, void* scratch, cudaStream_t st) {
-  if (n <= 0) return;
-  uint32_t* ka = (uint32_t*)scratch;
+cudaError_t scene_build_launch(const float* verts, const float* nrms, int n, float4* tri,
+                               float4* nrm, float4* geo, float4* mt, float4* nodes,
+                               void* scratch, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  float4* blo_a = (float4*)scratch;
+  float4* bhi_a = blo_a + n;
+  float4* blo_b = bhi_a + n;
+  float4* bhi_b = blo_b + n;
+  uint32_t* ka = (uint32_t*)(bhi_b + n);
   uint32_t* kb = ka + n;
   uint32_t* va = kb + n;
   uint32_t* vb = va + n;
   uint32_t* hist = vb + n;
   uint32_t* bb = hist + sort_hist_words(n);
-  int* child = (int*)(bb + 16);
-  int* parent = child + 2 * (size_t)n;
-  unsigned* flags = (unsigned*)(parent + 2 * (size_t)n);
+  int* cid_a = (int*)(bb + 16);
+  int* cid_b = cid_a + n;
+  int* nn = cid_b + n;
+  uint32_t* mflag = (uint32_t*)(nn + n);
+  uint32_t* keep = mflag + n;
+  uint32_t* mrank = keep + n;
+  uint32_t* kpos = mrank + n;
+  uint32_t* sums = kpos + n;
+  int* out = (int*)(sums + scan_tiles(n));
   const int tb = 256;
   const int gb = (n + tb - 1) / tb;
   face_setup_kernel<<<gb, tb, 0, st>>>(verts, nrms, n, tri, nrm, geo);
@@ -221,14 +279,36 @@ void scene_build_launch(const float* verts, const float* nrms, int n,
   scene_bbox_kernel<<<min(gb, 1184), tb, 0, st>>>(tri, n, bb);
   tri_morton_kernel<<<gb, tb, 0, st>>>(tri, n, bb, ka, va);
   const bool in_b = radix_sort_pairs<uint32_t>(ka, va, kb, vb, n, 30, hist, st);
-  const uint32_t* codes = in_b ? kb : ka;
   const uint32_t* order = in_b ? vb : va;
   leaf_setup_kernel<<<gb, tb, 0, st>>>(tri, n, order, mt);
-  if (n == 1) return;
-  radix_tree_kernel<<<(n - 1 + tb - 1) / tb, tb, 0, st>>>(codes, n, child,
-                                                          parent);
-  cudaMemsetAsync(flags, 0, (size_t)(n - 1) * sizeof(unsigned), st);
-  refit_kernel<<<gb, tb, 0, st>>>(mt, n, child, parent, flags, nodes, bb);
+  if (n == 1) return cudaGetLastError();
+  ploc_leaf_kernel<<<gb, tb, 0, st>>>(mt, n, bb, cid_a, blo_a, bhi_a);
+  int m = n, top = n - 1;
+  int counts[2] = {0, 0};
+  cudaError_t e;
+  // every pass merges at least one pair: at most n - 1 passes
+  for (int pass = 0; m > 1 && pass < n; ++pass) {
+    const int g = (m + tb - 1) / tb;
+    ploc_nn_kernel<<<(m + kPlocBlock - 1) / kPlocBlock, kPlocBlock, 0, st>>>(blo_a, bhi_a, m,
+                                                                             nn);
+    ploc_flags_kernel<<<g, tb, 0, st>>>(nn, m, mflag, keep);
+    exclusive_scan_u32(mflag, mrank, m, sums, st);
+    exclusive_scan_u32(keep, kpos, m, sums, st);
+    ploc_merge_kernel<<<g, tb, 0, st>>>(cid_a, blo_a, bhi_a, nn, m, mflag, mrank, keep, kpos, top,
+                                        cid_b, blo_b, bhi_b, nodes, out);
+    if ((e = cudaMemcpyAsync(counts, out, sizeof(counts), cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaStreamSynchronize(st)))
+      return e;
+    if (counts[1] < 1 || counts[1] > top || counts[0] != m - counts[1])
+      return cudaErrorUnknown;  // no progress: cannot happen with the tie rule
+    m = counts[0];
+    top -= counts[1];
+    std::swap(cid_a, cid_b);
+    std::swap(blo_a, blo_b);
+    std::swap(bhi_a, bhi_b);
+  }
+  if (m != 1 || top != 0) return cudaErrorUnknown;
+  return cudaGetLastError();
 }
 
 // Batched closest-hit queries (Scene::intersect, scene.h:307-348).

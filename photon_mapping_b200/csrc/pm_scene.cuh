@@ -1,4 +1,4 @@
-// Device scene: triangles, materials, area lights and the LBVH that
+// Device scene: triangles, materials, area lights and the BVH that
 // replaces the reference's Embree scene (scene.h:275-348).
 //
 // Layout in HBM (n faces, the reference's per-face unshared vertices):

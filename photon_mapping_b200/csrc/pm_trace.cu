@@ -292,7 +292,9 @@ void batch_trace_launch(const BatchTables& t, int64_t total_emit, int block, int
   const long long cap = (long long)sm_count() * (2048 / block);
   const unsigned gb = (unsigned)std::min<long long>(cap, (total_emit + block - 1) / block);
   cudaMemsetAsync(t.next_photon, 0, sizeof(unsigned long long), st);
-  if (stack <= 32)
+  if (stack <= 16)
+    batch_trace_kernel<16><<<gb, block, 0, st>>>(t, total_emit);
+  else if (stack <= 32)
     batch_trace_kernel<32><<<gb, block, 0, st>>>(t, total_emit);
   else
     batch_trace_kernel<64><<<gb, block, 0, st>>>(t, total_emit);
