@@ -32,6 +32,9 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
   return m;
 }
+// lanemask_lt from a lane number already in a register (two integer
+// instructions instead of a special-register read).
+__device__ __forceinline__ unsigned lt_mask(int lane) { return (1u << lane) - 1u; }
 __device__ __forceinline__ unsigned lanemask_le() {
   unsigned m;
   asm("mov.u32 %0, %%lanemask_le;" : "=r"(m));

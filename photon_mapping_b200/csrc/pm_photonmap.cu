@@ -451,7 +451,7 @@ __device__ __forceinline__ bool select_kth_hist(const float4* pos4,
       in = min(255, __float2int_rz(__fmul_rz(__uint_as_float(s.key[i]), sc))) ==
            bin;
     const unsigned bal = __ballot_sync(kFull, in);
-    if (in) s.sel[pos + __popc(bal & lanemask_lt())] = (uint32_t)i;
+    if (in) s.sel[pos + __popc(bal & lt_mask(lane))] = (uint32_t)i;
     pos += __popc(bal);
   }
   __syncwarp();
@@ -533,7 +533,7 @@ __device__ __forceinline__ int compact_kept(const float4* pos4, WarpBuf<C>& s,
     const unsigned bal = __ballot_sync(kFull, kp);
     __syncwarp();
     if (kp) {
-      const int o = dst + __popc(bal & lanemask_lt());
+      const int o = dst + __popc(bal & lt_mask(lane));
       s.key[o] = key;
       s.id[o] = id;
     }
@@ -573,7 +573,7 @@ __device__ __forceinline__ void offer(const MapDev& m, Query& q, WarpBuf<C>& s,
   const bool pass = valid && d2 <= q.tau;
   const unsigned bal = __ballot_sync(kFull, pass);
   if (pass) {
-    const int o = q.cnt + __popc(bal & lanemask_lt());
+    const int o = q.cnt + __popc(bal & lt_mask(lane));
     s.key[o] = __float_as_uint(d2);
     s.id[o] = (uint32_t)i;
   }
@@ -659,7 +659,7 @@ __device__ __forceinline__ void collect(const MapDev& m, const Levels& L,
     const float4 hi = __ldg(m.boxes + 2 * jb + 1);
     const bool pass = in && box_dist2(q.x, q.y, q.z, lo, hi) <= q.tau;
     const unsigned bal = __ballot_sync(kFull, pass);
-    const int off = __popc(bal & lanemask_lt());
+    const int off = __popc(bal & lt_mask(lane));
     if (cl == 0) {
       // the passing groups join the waiting list
       if (pass) s.list[pending + off] = (uint32_t)c;

@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(kSortThreads)
     }
     const uint32_t d = ok ? ((uint32_t)(key >> shift) & 255u) : 0xffffffffu;
     const unsigned peers = __match_any_sync(kFull, d);
-    const unsigned rank = __popc(peers & lanemask_lt());
+    const unsigned rank = __popc(peers & lt_mask(tid & 31));
     if (ok && rank == 0) wcnt[warp][d] = __popc(peers);
     __syncthreads();
     if (ok) {

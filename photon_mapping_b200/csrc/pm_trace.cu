@@ -210,7 +210,7 @@ __device__ __forceinline__ void trace_persistent(unsigned long long* next, long 
       if (lane == leader) base = atomicAdd(next, (unsigned long long)__popc(want));
       base = __shfl_sync(kFull, base, leader);
       if (!live && !done) {
-        g = (long long)(base + (unsigned)__popc(want & lanemask_lt()));
+        g = (long long)(base + (unsigned)__popc(want & lt_mask(lane)));
         if (g < total) {
           const int i = first(g, src);
           photon_emit<MODE>(scene(src), args(src), i, p);
