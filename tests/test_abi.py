@@ -56,6 +56,10 @@ def test_status_strings_and_null_context(lib_path):
     # null context: an argument error, never a crash
     assert lib.pm_ctx_synchronize(None) == 1
     assert lib.pm_photonmap_build(None, 0, None, ctypes.c_int64(0)) == 1
+    # null batch: the same
+    assert lib.pm_batch_render(None, 0, None) == 1
+    assert lib.pm_batch_photons(None, 0, None) == 1
+    assert lib.pm_batch_stage_times(None, None, 6) == 1
 
 
 def test_radiance_query_record_is_48_bytes():

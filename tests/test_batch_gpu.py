@@ -67,6 +67,20 @@ def test_autotune_keeps_the_images(batch_and_reference):
         np.testing.assert_array_equal(br.image(i), want[i])
 
 
+def test_stage_times_cover_a_step(batch_and_reference):
+    """pm_batch_stage_times runs one step stage by stage: six positive times
+    whose sum is about one step's device time, and the images of that step
+    are the per-scene loop's."""
+    scenes, br, want, _ = batch_and_reference
+    step = min(br.render(use_graph=False) for _ in range(3))
+    st = br.stage_times()
+    assert list(st) == ["trace", "maps", "camera", "sort", "knn", "resolve"]
+    assert all(v > 0.0 for v in st.values()), st
+    assert 0.5 * step < sum(st.values()) < 2.0 * step + 1.0, (st, step)
+    for i in range(len(scenes)):
+        np.testing.assert_array_equal(br.image(i), want[i])
+
+
 def test_batch_errors(batch_and_reference):
     scenes, br, _, _ = batch_and_reference
     with pytest.raises(PMError):
