@@ -316,6 +316,7 @@ int plan_maps(pm_batch* b) {
   a.n_scenes = n;
   a.scene_bits = bits_for(n);
   a.max_levels = max_levels;
+  a.num_sms = b->num_sms;
   return PM_OK;
 }
 

