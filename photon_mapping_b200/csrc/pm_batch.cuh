@@ -1,6 +1,6 @@
 // Batched rendering of many scenes: the per-scene tables the batched
 // kernels read and their launchers (pm_trace.cu, pm_render.cu,
-// pm_photonmap.cu). Each batched kernel covers every scene of the batch in
+// pm_photonmap.cu, pm_batch_maps.cu). Each batched kernel covers every scene of the batch in
 // one launch; a thread or warp finds its scene by binary search in a prefix
 // array (pixels, emitted photons, query work items) held in shared memory.
 #pragma once
