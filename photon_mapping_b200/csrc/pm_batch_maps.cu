@@ -249,6 +249,7 @@ __global__ void __launch_bounds__(kSegThreads)
   }
 }
 
+// out[j] = trace record order[j] (one scene's photon vector, on demand).
 __global__ void __launch_bounds__(kSegThreads)
     seg_photons_kernel(const float* __restrict__ raw, const uint32_t* __restrict__ order,
                        int64_t m, float* __restrict__ out) {
@@ -289,12 +290,13 @@ void batch_maps_launch(const BatchMapBuild& a, cudaStream_t st) {
   // narrow window of index-order places, so the scattered 12-B writes fill
   // their sectors in L2 before eviction (48.2 -> 37.5 ms for the maps of 211M
   // photons against 16 blocks per SM)
-  seg_place_kernel<<<grid_for(total, tb, a.num_sms, 4), tb, 0, st>>>(a.keys_a, a.raw, total, a.stored_off, a.emit_off, n,
-                                      a.first, a.bb, a.keys_b, a.order, a.va, a.err);
-  const bool in_a = radix_sort_pairs<unsigned long long>(a.keys_b, a.va, a.keys_a, a.vb,
-                                                         (int)total, 30 + a.scene_bits, a.hist,
-                                                         st);
-  const uint32_t* perm = in_a ? a.vb : a.va;
+  seg_place_kernel<<<grid_for(total, tb, a.num_sms, 4), tb, 0, st>>>(
+      a.keys_a, a.raw, total, a.stored_off, a.emit_off, n, a.first, a.bb, a.keys_b, a.order,
+      a.va, a.err);
+  // sorted pairs end in (keys_a, vb) or back in (keys_b, va)
+  const bool in_second = radix_sort_pairs<unsigned long long>(
+      a.keys_b, a.va, a.keys_a, a.vb, (int)total, 30 + a.scene_bits, a.hist, st);
+  const uint32_t* perm = in_second ? a.vb : a.va;
   // 3. the map arrays
   seg_gather_kernel<<<gb, tb, 0, st>>>(a.raw, a.order, perm, total, a.stored_off, n, a.pos4,
                                        a.thr4, a.wi2);
