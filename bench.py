@@ -35,7 +35,7 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 K_NEAREST = 100
-N_EMIT = 1_000_000          # photons emitted for the global map (config 2)
+N_EMIT = 1_000_000          # photons emitted for the global map of the benchmark
 TRACE_SEED = 1
 MAX_DEPTH = 100
 IMAGE_W = IMAGE_H = 512
@@ -59,9 +59,11 @@ def parse_args():
     ap.add_argument("--no-grad", action="store_true", help="skip the gradient measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-render measurements")
     ap.add_argument("--batch-scenes", type=int, default=64)
-    ap.add_argument("--convergence", type=int, nargs="*", default=None, metavar="CONFIG",
+    ap.add_argument("--convergence", nargs="*", default=None, metavar="NAME",
                     help="instead of the benchmark: image error against the path tracer for "
-                         "these configs (default 1 2 3), beside the reference integrator's")
+                         "these settings of photon_mapping_b200.configs (default all: "
+                         "cornell-256, cornell-512-final-gathering, caustics-512), beside the "
+                         "reference integrator's")
     ap.add_argument("--pt-spp", type=int, default=4096)
     ap.add_argument("--trace-render", choices=["cornell", "caustics"], default=None,
                     help="instead of the benchmark: trace the photon maps of this scene twice "
@@ -728,20 +730,20 @@ REF_BAND_BUDGET_S = 20.0
 
 
 def run_convergence(args) -> None:
-    """One JSON line per config: the device render's error against the
+    """One JSON line per render setting: the device render's error against the
     path-traced image (photon_mapping_b200.configs), and on a band of rows
     the same error of the reference's own PhotonMapping (its own photon
     tracing and camera pass, oracle/_ref, on the host cores) against the
     same path-traced image. The reference integrator has one gather ray per
-    hit, so configs with more are reported without it."""
+    hit, so settings with more are reported without it."""
     from oracle import oracle as O
     from photon_mapping_b200 import Context
     from photon_mapping_b200 import configs as CF
     from photon_mapping_b200 import scene as S
     ctx = Context(0)
-    for num in (args.convergence or sorted(CF.CONFIGS)):
-        rec, img, pt = CF.run_config(ctx, num, args.pt_spp, return_images=True)
-        c = CF.CONFIGS[num]
+    for name in (args.convergence or CF.NAMES):
+        rec, img, pt = CF.run_config(ctx, name, args.pt_spp, return_images=True)
+        c = CF.CONFIGS[name]
         rec["reference"] = None
         if c["n_gather"] == 1 and O.ref_integrator_available():
             with tempfile.TemporaryDirectory() as td:

@@ -2,9 +2,10 @@
 image-convergence measurement: a photon-mapping render of each against a
 path-traced render of the same scene at high sample count.
 
-    python -m photon_mapping_b200.configs [--config 1 2 3] [--pt-spp 4096]
+    python -m photon_mapping_b200.configs [--config NAME ...] [--pt-spp 4096]
 
-prints one JSON line per config: render and photon-trace times, samples/s,
+(NAME: cornell-256, cornell-512-final-gathering, caustics-512; all three by
+default) prints one JSON line per setting: render and photon-trace times, samples/s,
 and the RMSE of the photon-mapping image against the path tracer
 (integrator.h:51-106 on the device) at 2 x pt-spp, on raw linear radiance
 over all pixels and channels. Also given: the same without pixels that see
@@ -26,13 +27,15 @@ from .camera import Camera
 MAX_DEPTH = 100
 
 CONFIGS = {
-    1: dict(name="cornell-256", scene="cornell", width=256, height=256, spp=16,
-            photons=100_000, caustics_multiplier=1.0, k=100, fg=0, n_gather=1),
-    2: dict(name="cornell-512-final-gathering", scene="cornell", width=512, height=512, spp=100,
-            photons=1_000_000, caustics_multiplier=1.0, k=100, fg=1, n_gather=16),
-    3: dict(name="caustics-512", scene="caustics", width=512, height=512, spp=64,
-            photons=1_000_000, caustics_multiplier=10.0, k=100, fg=1, n_gather=1),
+    "cornell-256": dict(scene="cornell", width=256, height=256, spp=16, photons=100_000,
+                        caustics_multiplier=1.0, k=100, fg=0, n_gather=1),
+    "cornell-512-final-gathering": dict(scene="cornell", width=512, height=512, spp=100,
+                                        photons=1_000_000, caustics_multiplier=1.0, k=100,
+                                        fg=1, n_gather=16),
+    "caustics-512": dict(scene="caustics", width=512, height=512, spp=64, photons=1_000_000,
+                         caustics_multiplier=10.0, k=100, fg=1, n_gather=1),
 }
+NAMES = list(CONFIGS)
 
 
 def make_scene(kind: str) -> S.Mesh:
@@ -96,15 +99,15 @@ def path_traced_reference(ctx, cam, width: int, height: int, spp: int):
     return both, noise, secs
 
 
-def run_config(ctx, num: int, pt_spp: int, spp: int | None = None, seed: int = 1,
+def run_config(ctx, name: str, pt_spp: int, spp: int | None = None, seed: int = 1,
                save_dir: str | None = None, return_images: bool = False):
-    """Traces and renders config `num` on `ctx`, path-traces the reference
+    """Traces and renders setting `name` of CONFIGS on `ctx`, path-traces the reference
     image, and returns the record printed by the command line (with
     return_images: the record, the photon-mapping image and the path-traced
     image). With save_dir, both images are written there as .npy (raw
     linear radiance)."""
     from .integrator import PhotonMapping
-    c = CONFIGS[num]
+    c = CONFIGS[name]
     spp = c["spp"] if spp is None else spp
     mesh = make_scene(c["scene"])
     sc = S.Scene(ctx)
@@ -125,11 +128,11 @@ def run_config(ctx, num: int, pt_spp: int, spp: int | None = None, seed: int = 1
     if save_dir:
         from pathlib import Path
         Path(save_dir).mkdir(parents=True, exist_ok=True)
-        np.save(Path(save_dir) / f"config{num}_photon_mapping.npy", img)
-        np.save(Path(save_dir) / f"config{num}_path_tracing.npy", ref)
+        np.save(Path(save_dir) / f"{name}_photon_mapping.npy", img)
+        np.save(Path(save_dir) / f"{name}_path_tracing.npy", ref)
     n = c["width"] * c["height"] * spp
     rec = {
-        "config": num, **c, "spp": spp, "triangles": int(mesh.n_faces),
+        "name": name, **c, "spp": spp, "triangles": int(mesh.n_faces),
         "photons_stored": {k: int(v["stored"]) for k, v in stats.items()},
         "trace_s": t_trace, "render_s": t_render, "samples_per_s": n / t_render,
         "render_stats": rst,
@@ -144,7 +147,7 @@ def main(argv=None) -> None:
     from . import Context
     ap = argparse.ArgumentParser(description=__doc__,
                                  formatter_class=argparse.RawDescriptionHelpFormatter)
-    ap.add_argument("--config", type=int, nargs="+", default=sorted(CONFIGS))
+    ap.add_argument("--config", nargs="+", choices=NAMES, default=NAMES)
     ap.add_argument("--pt-spp", type=int, default=4096,
                     help="the path-traced reference uses twice this many samples")
     ap.add_argument("--spp", type=int, default=None, help="override the config's spp")
@@ -152,8 +155,8 @@ def main(argv=None) -> None:
     ap.add_argument("--save", default=None, help="directory for the images (.npy)")
     args = ap.parse_args(argv)
     ctx = Context(args.device)
-    for num in args.config:
-        print(json.dumps(run_config(ctx, num, args.pt_spp, args.spp, save_dir=args.save)), flush=True)
+    for name in args.config:
+        print(json.dumps(run_config(ctx, name, args.pt_spp, args.spp, save_dir=args.save)), flush=True)
     ctx.close()
 
 

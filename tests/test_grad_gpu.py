@@ -75,7 +75,7 @@ def test_gradient_matches_oracle_fp64(ctx, fg, n_gather, md):
 
 
 def test_gradient_matches_finite_differences(ctx):
-    """Config-4 shape at reduced size: Cornell box, final gathering, k = 50,
+    """The gradient benchmark's shape at reduced size: Cornell box, final gathering, k = 50,
     full path depth (Russian roulette active, decisions frozen)."""
     mesh0 = S.cornell_box(0)
     r = D.DiffRenderer(ctx, mesh0, camera(), 48, 48, 4, 100000, 50, final_gathering_depth=1,
