@@ -65,6 +65,10 @@ def parse_args():
                          "cornell-256, cornell-512-final-gathering, caustics-512), beside the "
                          "reference integrator's")
     ap.add_argument("--pt-spp", type=int, default=4096)
+    ap.add_argument("--batch-stages", type=int, default=None, metavar="N",
+                    help="instead of the benchmark: build a batch of the first N random scenes "
+                         "of the batched leg and print one step's stage times (a short run "
+                         "for profiling the batched kernels)")
     ap.add_argument("--trace-render", choices=["cornell", "caustics"], default=None,
                     help="instead of the benchmark: trace the photon maps of this scene twice "
                          "(1M global photons, caustics x10 with the caustics scene) and render "
@@ -852,9 +856,21 @@ def run_trace_render(args) -> None:
     ctx.close()
 
 
+def run_batch_stages(args) -> None:
+    from photon_mapping_b200 import batch as B
+    scenes = [B.random_scene(1000 + s) for s in range(args.batch_stages)]
+    br = B.BatchRenderer(scenes)
+    stored, queries = br.counts()
+    print(json.dumps({"scenes": len(scenes), "photons_stored": int(stored.sum()),
+                      "queries": int(queries.sum()), "stage_ms": br.stage_times()}), flush=True)
+    br.close()
+
+
 def main():
     args = parse_args()
-    if args.trace_render is not None:
+    if args.batch_stages is not None:
+        run_batch_stages(args)
+    elif args.trace_render is not None:
         run_trace_render(args)
     elif args.convergence is not None:
         run_convergence(args)
