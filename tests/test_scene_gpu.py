@@ -1,4 +1,4 @@
-"""Parity of the device scene (LBVH closest hit) and of the photon tracer
+"""Parity of the device scene (BVH closest hit) and of the photon tracer
 with the CPU oracle.
 
 Bar: closest hits identical (t, u, v and face index, bit for bit) to a
@@ -65,6 +65,63 @@ def test_cornell_intersections_exact(ctx):
     want = O.OracleScene(mesh).intersect(rays8(o, d))
     check_hits(got, want)
     assert (got["prim"] >= 0).mean() > 0.5
+
+
+def _edge_case_mesh(kind: str) -> S.Mesh:
+    """Small or tie-heavy scenes for the clustering build (pm_scene.cu):
+    the fewest faces with an inner node, duplicates (equal boxes and equal
+    hit distances), zero-area faces, one face far larger than the rest, and
+    faces whose boxes are all the same cube."""
+    seeds = {"two": 1, "three": 2, "duplicates": 3, "zero_area": 4, "huge_and_tiny": 5,
+             "equal_boxes": 6}
+    rng = np.random.default_rng(seeds[kind])
+
+    def tris(n, lo=0.0, hi=1.0, size=0.2):
+        c = rng.uniform(lo, hi, (n, 1, 3))
+        return (c + rng.uniform(-size, size, (n, 3, 3))).reshape(n, 9)
+
+    if kind == "two":
+        t = tris(2)
+    elif kind == "three":
+        t = tris(3)
+    elif kind == "duplicates":
+        t = np.concatenate([np.repeat(tris(1), 300, axis=0), tris(5)])
+    elif kind == "zero_area":
+        a = rng.uniform(0, 1, (200, 3))
+        b = rng.uniform(0, 1, (200, 3))
+        line = np.concatenate([a, b, 0.5 * (a + b)], axis=1)  # collinear vertices
+        t = np.concatenate([line, tris(200)])[rng.permutation(400)]
+    elif kind == "huge_and_tiny":
+        big = np.array([[-10.0, -10.0, 0.5, 10.0, -10.0, 0.5, 0.0, 10.0, 0.5]])
+        t = np.concatenate([tris(5000, size=0.01), big])
+    elif kind == "equal_boxes":
+        third = rng.uniform(0.05, 0.95, (1000, 3))
+        t = np.concatenate([np.zeros((1000, 3)), np.ones((1000, 3)), third], axis=1)
+    else:
+        raise ValueError(kind)
+    up = np.tile(np.array([0.0, 0.0, 1.0]), (t.shape[0], 3))  # zero-area faces have no normal
+    return S.mesh_from_triangles(t.astype(np.float64), S.material(rho=S.WHITE), "white",
+                                 normals=up)
+
+
+@pytest.mark.parametrize("kind", ["two", "three", "duplicates", "zero_area", "huge_and_tiny",
+                                  "equal_boxes"])
+def test_bvh_edge_case_scenes_exact(ctx, kind):
+    mesh = _edge_case_mesh(kind)
+    sc = S.Scene(ctx)
+    sc.setMesh(mesh)
+    sc.build()
+    rng = np.random.default_rng(7)
+    o, d = random_rays(rng, 20000)
+    o2 = rng.uniform(0, 1, (2000, 3)).astype(np.float32)
+    d2 = np.zeros((2000, 3), np.float32)
+    d2[np.arange(2000), rng.integers(0, 3, 2000)] = rng.choice([-1.0, 1.0], 2000)
+    o = np.concatenate([o, o2])
+    d = np.concatenate([d, d2])
+    got = sc.intersect(o, d)
+    want = O.OracleScene(mesh).intersect(rays8(o, d))
+    check_hits(got, want)
+    assert (got["prim"] >= 0).sum() > 0
 
 
 def test_shadow_ray_tmax_and_misses(ctx):
