@@ -81,6 +81,37 @@ def test_stage_times_cover_a_step(batch_and_reference):
         np.testing.assert_array_equal(br.image(i), want[i])
 
 
+def test_batch_scenes_with_no_or_few_photons():
+    """The segmented map build with empty and nearly empty maps among full
+    ones: a scene that emits no photons (its estimates are 0), scenes whose
+    few stored photons fill less than one 8-photon group, and ordinary
+    scenes. Images bit-identical to the per-scene loop; stored counts equal."""
+    base = dict(tri_range=(600, 5000), side_range=(16, 40), ks=(10, 40), spp=2, max_depth=20)
+    scenes = []
+    for s, photons in enumerate([0, 1, 3, 20000, 7, 30000]):
+        sc = B.random_scene(50 + s, photon_range=(1000, 2000), **base)
+        sc["photons"] = photons
+        scenes.append(sc)
+    seq = B.Sequential(scenes)
+    want, _ = seq.render()
+    stored_seq = [pmi.stats["global"]["stored"] for pmi in seq.pmis]
+    seq.close()
+    br = B.BatchRenderer(scenes)
+    try:
+        stored, _ = br.counts()
+        assert list(stored) == stored_seq
+        assert stored[0] == 0
+        for use_graph in (False, True):
+            br.render(use_graph=use_graph)
+            for i in range(len(scenes)):
+                np.testing.assert_array_equal(br.image(i), want[i])
+        for i in (1, 2, 4):
+            ph = br.photons(i)
+            assert ph.shape == (stored[i], 9)
+    finally:
+        br.close()
+
+
 def test_batch_errors(batch_and_reference):
     scenes, br, _, _ = batch_and_reference
     with pytest.raises(PMError):
