@@ -688,7 +688,7 @@ int pm_batch_autotune(pm_batch* b, pm_batch_tuning* best, float* ms_stage) {
   // kNN: warps x chunk x buffer
   float best_knn = 3.4e38f;
   const int warps[] = {4, 8};
-  const int chunks[] = {8, 16, 32, 64};
+  const int chunks[] = {8, 16, 32, 64, 128, 256, 512, 1024};
   const int bufs[] = {512, 2048};
   for (int w : warps)
     for (int c : chunks)
